@@ -1,0 +1,178 @@
+/*
+ * psipm_b200 — B200-native normal-equations inner solve for PS-IPM / HSD.
+ *
+ * C ABI of libpsipm_b200.so.  Plain pointers and sizes only; every array
+ * argument is HOST memory unless the function name ends in _dev.  One handle
+ * owns one LP's device data (A, A^T, weights, core, factor, PCG workspace)
+ * and one CUDA stream; calls on a handle must come from one host thread at a
+ * time and are synchronous on return.
+ *
+ * The operations replace the arithmetic of the reference's KKT solver
+ * objects (StefanoCipolla/MF-PSIPM):
+ *   SpectralStableColumnPreconditioner   psipm_spectral_preconditioner.py:143-752
+ *   StableActiveColumnPreconditioner     psipm_stable_preconditioner.py:113-517
+ *   NormalEquations (factor/apply)       psipm_active_pool.py:720-996
+ *   V3.1 _pcg / HSDNewtonSystem.matvec   psipm_v3_1_hsd.py:1015-1063, 1136-1137
+ * The refresh/refactor policy, statistics and exceptions of those classes
+ * stay in the host wrapper (psipm_b200/kkt.py), which maps every nonzero
+ * status to the reference's KKTSolveError.
+ */
+#ifndef PSIPM_B200_H
+#define PSIPM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define PSIPM_OK 0
+#define PSIPM_ERR_ARGUMENT (-1)   /* invalid size, pointer or option */
+#define PSIPM_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define PSIPM_ERR_NOT_PD (-3)     /* Cholesky failed at every diagonal shift */
+#define PSIPM_ERR_STATE (-4)      /* call order (e.g. apply before factor) */
+#define PSIPM_ERR_BOUNDS (-5)     /* a device index check tripped */
+#define PSIPM_ERR_TIMEOUT (-6)    /* a device loop hit its deadline */
+#define PSIPM_ERR_MEMORY (-7)     /* device allocation failed */
+#define PSIPM_ERR_SYMBOLIC (-8)   /* symbolic analysis rejected the pattern */
+#define PSIPM_ERR_UNSUPPORTED (-9)
+
+typedef struct psipm_handle psipm_handle;
+
+/* PCG variants (the two reference loops) */
+#define PSIPM_PCG_SPECTRAL 0 /* psipm_spectral_preconditioner.py:469-581 */
+#define PSIPM_PCG_HSD 1      /* psipm_v3_1_hsd.py:1015-1063 */
+
+/* precision of the PCG inner iterations */
+#define PSIPM_FP64 0       /* everything in FP64 */
+#define PSIPM_FP32_REFINED 1 /* FP32 SpMV/factor/solves, FP64 true residual + refinement */
+
+typedef struct {
+    int32_t info;            /* reference KrylovResult.info: 0 ok, >0 limit, -1..-7 breakdown */
+    int32_t iterations;      /* PCG iterations (sum over refinement sweeps) */
+    int32_t matvecs;         /* H·p products, true-residual ones included */
+    int32_t replacements;    /* residual replacements */
+    int32_t residual_checks; /* true-residual verifications */
+    int32_t n_alpha;         /* entries written to alphas[] (current Lanczos run) */
+    int32_t n_beta;          /* entries written to betas[] */
+    int32_t n_history;       /* entries written to history[] */
+    int32_t refinements;     /* FP64 refinement sweeps (FP32_REFINED only) */
+    int32_t ok;              /* HSD variant: converged flag */
+    double relative_residual;/* ||rhs - H x|| / max(1, ||rhs||) in FP64 */
+    double seconds;          /* device time of the call (CUDA events) */
+} psipm_pcg_info;
+
+typedef struct {
+    int32_t nsupernodes;
+    int32_t nlevels;
+    int32_t max_front;
+    int32_t symbolic_analyses; /* cumulative */
+    int64_t nnz_factor;        /* stored entries of L */
+    double flops;              /* numeric factorisation flops */
+    double symbolic_seconds;   /* last host symbolic analysis */
+    double factor_seconds;     /* last numeric factorisation (device) */
+} psipm_factor_info;
+
+/* ---- lifetime -------------------------------------------------------------
+ * A is m x n in CSC (colptr[n+1], rowidx[nnz], values[nnz]); indices sorted
+ * within columns, no duplicates (the reference canonicalises A the same way,
+ * psipm_active_pool.py:781-784).  Replaces NormalEquations.__init__ and the
+ * candidate bookkeeping of StableActiveColumnPreconditioner.__init__
+ * (psipm_stable_preconditioner.py:162-201).  `device` is the CUDA ordinal. */
+int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr,
+                 const int32_t* rowidx, const double* values, int32_t device,
+                 int32_t precision, psipm_handle** out);
+void psipm_destroy(psipm_handle* h);
+const char* psipm_last_error(const psipm_handle* h);
+
+/* Number and (global, ascending) indices of the candidate columns: columns
+ * with at least two nonzeros (psipm_stable_preconditioner.py:169-172). */
+int64_t psipm_num_candidates(const psipm_handle* h);
+int psipm_get_candidates(const psipm_handle* h, int64_t* out);
+
+/* ---- weights ----------------------------------------------------------------
+ * theta[n] (host).  Stores theta and w = 1/theta on the device; replaces
+ * `self._weights = 1.0 / theta` (psipm_stable_preconditioner.py:399) and the
+ * `self.theta = theta` of every factorize. */
+int psipm_set_theta(psipm_handle* h, const double* theta, double delta);
+
+/* ---- S3 leverage scores -----------------------------------------------------
+ * scores[ncand] = w_C * (A2_C^T (1/max(A2 w + max(delta,tiny), tiny))) /
+ * (1 + fill_weight * q(q-1)/2), bit-identical to _scores
+ * (psipm_stable_preconditioner.py:293-309).  Either output may be NULL. */
+int psipm_scores(psipm_handle* h, double fill_weight, double* scores, double* diagonal);
+
+/* ---- S1/S4 core refresh -----------------------------------------------------
+ * New core from the current scores, as _refresh_core does
+ * (psipm_stable_preconditioner.py:311-371): mandatory columns, the top
+ * floor(retention*target) of the old core (if stable), trimming, and the top
+ * remaining candidates; ties broken by candidate index.  mandatory_local are
+ * sorted candidate-local positions.  core_out (capacity ncand) receives the
+ * sorted global column indices; *retained the fraction of the old core kept.
+ * psipm_scores must have been called for the current weights. */
+int psipm_refresh_core(psipm_handle* h, int64_t target, double retention, int32_t stable,
+                       const int64_t* mandatory_local, int64_t nmandatory,
+                       int64_t* core_out, int64_t* ncore, double* retained);
+/* Install an explicit core (sorted global column indices). */
+int psipm_set_core(psipm_handle* h, const int64_t* core, int64_t ncore);
+/* Top-`count` candidates among those with mask[i]!=0 (NULL mask: all) by
+ * (score desc, index asc), finite scores only — the reference's _top_k
+ * (psipm_stable_preconditioner.py:97-110) — written as ascending local
+ * indices to out (capacity count); *nout receives how many. */
+int psipm_top_k(psipm_handle* h, const double* scores, int64_t nscores, const uint8_t* mask,
+                int64_t count, int64_t* out, int64_t* nout);
+
+/* ---- F1/F2 factor -------------------------------------------------------------
+ * Assemble P = A_C diag(w_C) A_C^T + diag(max(A2 w - diag_C, 0) + delta),
+ * Jacobi-scale it to unit diagonal and factor it on the device, trying the
+ * diagonal shifts (0,1e-14,...,1e-2) from index `start_shift` on
+ * (psipm_active_pool.py:839-897).  The symbolic analysis is redone when the
+ * core changed since the last one.  *shift_index receives the shift used. */
+int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* shift_index,
+                 psipm_factor_info* info);
+
+/* ---- H4 preconditioner apply: z = P^{-1} r (psipm_active_pool.py:903-904) */
+int psipm_apply(psipm_handle* h, const double* r, double* z);
+
+/* ---- H3 operator: y = A diag(w) A^T v + delta v
+ * (psipm_stable_preconditioner.py:434-438, psipm_v3_1_hsd.py:1136-1137) */
+int psipm_matvec(psipm_handle* h, const double* v, double* y);
+
+/* ---- H2/H2b PCG on H with P as preconditioner ---------------------------------
+ * variant PSIPM_PCG_SPECTRAL restates psipm_spectral_preconditioner.py:469-581
+ * (initial guess P^{-1} rhs, residual replacement every `replacement`
+ * iterations, breakdown codes); PSIPM_PCG_HSD restates psipm_v3_1_hsd.py:1015-1063.
+ * alphas/betas (capacity maxit) receive the current Lanczos run,
+ * history (capacity maxit+2) the explicit relative residuals; any may be NULL.
+ * residual (m, may be NULL) receives rhs - H x. */
+int psipm_pcg(psipm_handle* h, const double* rhs, double tol, int32_t maxit, int32_t variant,
+              int32_t replacement, double gap_tolerance, double* x, double* residual,
+              double* alphas, double* betas, double* history, psipm_pcg_info* info);
+
+/* ---- H1 Newton solve ------------------------------------------------------------
+ * w = r1/theta; rhs = r2 - A w; dy = PCG(rhs); dx = w + (A^T dy)/theta
+ * (psipm_spectral_preconditioner.py:651-752 without the host policy). */
+int psipm_solve(psipm_handle* h, const double* r1, const double* r2, double tol, int32_t maxit,
+                int32_t variant, int32_t replacement, double gap_tolerance, double* dx,
+                double* dy, double* residual, double* alphas, double* betas, double* history,
+                psipm_pcg_info* info);
+
+/* ---- device-pointer variants (no host copies) ----------------------------------- */
+int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev, double tol,
+                    int32_t maxit, int32_t variant, int32_t replacement, double gap_tolerance,
+                    double* dx_dev, double* dy_dev, psipm_pcg_info* info);
+
+/* ---- diagnostics ---------------------------------------------------------------- */
+/* Kernels launched by this handle since creation (all of them are this
+ * library's own kernels). */
+int64_t psipm_kernel_launches(const psipm_handle* h);
+/* Time of the last PCG's phases on the device (seconds): [0] H·p,
+ * [1] preconditioner apply, [2] vector ops; filled only when profiling is on. */
+int psipm_set_profiling(psipm_handle* h, int32_t on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSIPM_B200_H */

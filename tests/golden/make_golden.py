@@ -1,0 +1,129 @@
+"""Generate the golden fixtures by running the unmodified reference.
+
+Run in a container that has the reference checked out (read-only) at
+``/root/reference`` or at the path given by ``--reference``:
+
+    python tests/golden/make_golden.py [--reference PATH]
+
+The reference needs ``sksparse.cholmod`` (CHOLMOD), which is not installed
+in this image; ``tests/golden/cholmod_standin`` provides the same API on top
+of SciPy's SuperLU and is put first on ``sys.path``.  So every fixture is
+"reference code + SuperLU stand-in factor".
+
+For each seeded instance the script wraps the reference's
+``SpectralStableColumnPreconditioner`` (psipm_spectral_preconditioner.py:143)
+so that every ``factorize`` and ``solve`` call records its inputs and
+outputs, runs ``psipm_solve`` (psipm_active_pool.py:2277) to tolerance 1e-8
+and writes ``<name>.npz`` next to this script: the LP, the first
+``KEEP_CALLS`` factorize/solve records (theta, delta, scores at refresh,
+core, r1, r2, dx, dy, PCG iterations and tolerance), every core the
+refreshes produced, and the final iterate and status.
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+KEEP_CALLS = 8
+
+INSTANCES = {
+    "random_m300": ("random_lp", dict(m=300, n=900, seed=0)),
+    "grid_20x25": ("grid_network", dict(rows=20, cols=25, seed=1000)),
+    "cover_m200": ("set_cover", dict(m=200, n=10_000, seed=2000)),
+}
+# the small instances use the stable core path (the exact-preconditioner
+# gate, psipm_stable_preconditioner.py:202-207, would otherwise switch it off)
+OPTIONS = dict(full_preconditioner_row_threshold=10)
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--only", default=None)
+    args = parser.parse_args()
+    sys.path.insert(0, os.path.join(HERE, "cholmod_standin"))
+    sys.path.insert(0, args.reference)
+    sys.path.insert(0, os.path.join(REPO, "mf-psipm_b200"))
+    import psipm_active_pool as PS
+    import psipm_spectral_preconditioner as SSP
+    from psipm_b200 import synthetic
+
+    class Recording(SSP.SpectralStableColumnPreconditioner):
+        def __init__(self, *a, **k):
+            super().__init__(*a, **k)
+            self.rec_factor = []
+            self.rec_solve = []
+            self.rec_cores = []
+            self._pending_scores = None
+
+        def _scores(self, weights, delta):
+            s = super()._scores(weights, delta)
+            self._pending_scores = (np.array(weights), float(delta), np.array(s))
+            return s
+
+        def _refresh_core(self, weights, delta, stable, force_backbone=False):
+            super()._refresh_core(weights, delta, stable, force_backbone)
+            self.rec_cores.append(self.core.copy())
+
+        def factorize(self, theta, delta):
+            self._pending_scores = None
+            core_before = self.core.copy()
+            super().factorize(theta, delta)
+            if len(self.rec_factor) < KEEP_CALLS:
+                self.rec_factor.append(dict(
+                    theta=np.array(theta), delta=float(delta), core_before=core_before,
+                    core=self.core.copy(), scores=(None if self._pending_scores is None
+                                                   else self._pending_scores[2]),
+                    factor_age=int(self.factor_age), core_target=int(self.core_target)))
+
+        def solve(self, r1, r2):
+            dx, dy = super().solve(r1, r2)
+            if len(self.rec_solve) < KEEP_CALLS:
+                self.rec_solve.append(dict(
+                    r1=np.array(r1), r2=np.array(r2), dx=np.array(dx), dy=np.array(dy),
+                    theta=np.array(self.theta), delta=float(self.delta), core=self.core.copy(),
+                    iterations=int(self.cg_iterations[-1]), tolerance=float(self.cg_tolerances[-1])))
+            return dx, dy
+
+    for name, (family, kwargs) in INSTANCES.items():
+        if args.only and name != args.only:
+            continue
+        lp0 = getattr(synthetic, family)(**kwargs)
+        lp = PS.StandardLP(c=lp0.c, A=lp0.A, b=lp0.b, u=lp0.u, pos=lp0.pos, box=lp0.box)
+        solver = Recording(lp.A, protected=~lp.pos, **OPTIONS)
+        sol = PS.psipm_solve(lp, kkt="spectral-stable-pcg", kkt_solver=solver, tol=1e-8, printlevel=0)
+        out = dict(
+            family=family, kwargs=repr(kwargs), options=repr(OPTIONS),
+            A_data=lp.A.data, A_indices=lp.A.indices, A_indptr=lp.A.indptr,
+            A_shape=np.array(lp.A.shape), b=lp.b, c=lp.c, u=lp.u, pos=lp.pos, box=lp.box,
+            x=sol.x, y=sol.y, z=sol.z, w=sol.w, obj=sol.obj, status=sol.status,
+            res_p=sol.res_p, res_d=sol.res_d, mu=sol.mu,
+            pcg_iterations=sol.pcg_iterations, cg_iterations=np.array(solver.cg_iterations),
+            core_sizes=np.array(solver.core_sizes), n_fact=solver.n_fact,
+            candidates=solver.candidates, matching_columns=solver.matching_columns,
+            n_factor_calls=len(solver.rec_factor), n_solve_calls=len(solver.rec_solve),
+            n_cores=len(solver.rec_cores),
+        )
+        for i, rec in enumerate(solver.rec_factor):
+            for key, value in rec.items():
+                if value is not None:
+                    out[f"f{i}_{key}"] = value
+        for i, rec in enumerate(solver.rec_solve):
+            for key, value in rec.items():
+                out[f"s{i}_{key}"] = value
+        for i, core in enumerate(solver.rec_cores):
+            out[f"core{i}"] = core
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{name}: {sol.status} obj {sol.obj!r} pcg {sol.pcg_iterations} "
+              f"-> {os.path.getsize(path) / 1e6:.2f} MB")
+
+
+if __name__ == "__main__":
+    main()
