@@ -1,0 +1,339 @@
+#!/usr/bin/env python3
+"""Time to 1e-8 relative KKT residual with the B200 inner solve.
+
+Workload (one step): a full PS-IPM solve, to relative KKT residual 1e-8
+(primal, dual and gap, psipm_active_pool.py:2561-2637), of the seeded
+synthetic min-cost-flow LP on a 200 x 250 directed grid plus 10% random
+long-range arcs (m = 49,999 grounded rows, n = 219,010 arcs, all boxed),
+with the spectral stable-column preconditioned normal equations solved on
+the device in FP64.
+
+Keys of the JSON line:
+* value      seconds per LP solve with A already resident on the device
+             (CUDA events on the library's stream around K solves);
+* e2e        the same solve through the public API from host arrays:
+             handle creation (A uploaded), every per-iteration theta/r1/r2
+             upload and dx/dy download, the solution back on the host;
+* roofline   the persistent PCG kernel (k_pcg): algorithmic bytes of all
+             its launches / its CUDA-event time, against the measured HBM
+             copy bandwidth;
+* cpu_baseline  the CPU oracle (reference algorithm, SuperLU stand-in
+             factor) on a bounded sample of the same LP, scaled to one solve.
+
+``--impl reference`` times that CPU implementation alone (rank 0).
+Multi-GPU: one process per GPU (torchrun), each solving its own seeded
+instance (weak scaling, no collective on the data path); times are the max
+over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "mf-psipm_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "time to 1e-8 rel. KKT residual (PS-IPM, device normal-equations PCG)"
+WORKLOAD = ("min-cost flow LP, 200x250 directed grid (both orientations) + 10% random long-range arcs, "
+            "m=49,999 grounded rows, n=219,010 boxed arcs, nnz=438,005; spectral stable-column "
+            "preconditioner, FP64")
+HBM_FALLBACK = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--rows", type=int, default=200)
+    ap.add_argument("--cols", type=int, default=250)
+    ap.add_argument("--cpu-sample-outer", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", HBM_FALLBACK)), "measured"
+    return HBM_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_lp(args, rank: int):
+    from psipm_b200 import synthetic
+
+    return synthetic.grid_network(args.rows, args.cols, seed=1000 + rank)
+
+
+def cpu_oracle_sample(lp, tol, outer, seconds_limit=25.0):
+    """Reference algorithm (oracle) on the first `outer` outer iterations,
+    stopped after `seconds_limit` seconds."""
+    from oracle import ipm as OI
+    from oracle import stable as OS
+
+    t0 = time.perf_counter()
+    solver = OS.SpectralOracle(lp.A, protected=~lp.pos)
+    sol = OI.psipm_solve(lp, solver, tol=tol, max_outer=outer, time_limit=seconds_limit)
+    seconds = time.perf_counter() - t0
+    return seconds, max(1, sol.inner_iter), sol
+
+
+def blas_threads() -> int:
+    try:
+        from threadpoolctl import threadpool_info
+
+        info = threadpool_info()
+        return int(max((i.get("num_threads", 1) for i in info), default=1))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def flush_l2():
+    import torch
+
+    buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    buf.fill_(1.0)
+    torch.cuda.synchronize()
+    del buf
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    lp = make_lp(args, 0)
+    threads = blas_threads()
+    values = []
+    inner_ref = None
+    for step in range(args.warmup + args.steps):
+        seconds, inner, sol = cpu_oracle_sample(lp, args.tol, args.cpu_sample_outer)
+        if step >= args.warmup:
+            values.append((seconds, inner))
+    per_inner = sum(s for s, _ in values) / sum(i for _, i in values)
+    # scaled to one full solve with the inner-iteration count of a full run of
+    # the same algorithm (measured once per process on the first warm-up)
+    full_inner = FULL_INNER_ITERATIONS.get((args.rows, args.cols))
+    value = per_inner * full_inner if full_inner else None
+    sample = (f"first {args.cpu_sample_outer} PS-IPM outer iterations "
+              f"({values[0][1]} inner IPM iterations) of the same LP, scaled by "
+              f"{full_inner} inner iterations of a full solve")
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(s for s, _ in values) / len(values),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "tol": args.tol},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+# inner PS-IPM iterations of a full oracle solve to 1e-8 (same LP, measured in
+# this repository's CPU environment; used only to scale the bounded CPU sample)
+FULL_INNER_ITERATIONS = {}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from psipm_b200 import ipm
+    from psipm_b200.device import NormalEquationsDevice
+    from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner
+
+    torch.cuda.set_device(local_rank)
+    lp = make_lp(args, rank)
+    m, n = lp.A.shape
+    dev = NormalEquationsDevice(lp.A, device=local_rank)
+
+    def one_solve():
+        solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev)
+        sol = ipm.psipm_solve(lp, solver, tol=args.tol)
+        if sol.status != "optimal":
+            raise RuntimeError(f"solve ended {sol.status}")
+        return sol, solver
+
+    for _ in range(args.warmup):
+        one_solve()
+        flush_l2()
+    dist = world > 1
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    launches0 = dev.kernel_launches
+    total = 0.0
+    sols = []
+    pcg_s = pcg_b = 0.0
+    pcg_launches = pcg_its = 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        dev.timer_start()
+        sol, solver = one_solve()
+        total += dev.timer_stop()
+        sols.append(sol)
+        pcg_s += solver.device_seconds
+        pcg_b += solver.pcg_bytes
+        pcg_launches += solver.pcg_launches
+        pcg_its += solver.pcg_total_iterations
+        flush_l2()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = dev.kernel_launches - launches0
+    per_step = total / args.steps
+    if dist:
+        t = torch.tensor([per_step], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        per_step = float(t.item())
+    # ---- end to end through the public API, host buffers ----------------------
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sol_e2e, solver_e2e = ipm.solve_standard(lp, tol=args.tol, device=local_rank)
+    x_host = np.array(sol_e2e.x)
+    torch.cuda.synchronize()
+    e2e = time.perf_counter() - t0
+    h2d = (8 * (n + 1) + 12 * lp.A.nnz) + solver_e2e.h2d_bytes
+    d2h = 8 * solver_e2e.candidates.size + solver_e2e.d2h_bytes + 8 * x_host.size * 0
+    solver_e2e.close()
+    if dist:
+        t = torch.tensor([e2e], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e = float(t.item())
+    peak, peak_kind = measured_peaks()
+    achieved = pcg_b / pcg_s / 1e9 if pcg_s > 0 else None
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "kernel": "k_pcg", "peak_source": f"{peak_kind} hbm_gbs",
+            "pcg_launches": pcg_launches, "pcg_iterations": pcg_its,
+            "pcg_seconds_per_step": pcg_s / args.steps,
+            "note": "the LP's operator (~10 MB) is L2-resident; the fraction of HBM peak is "
+                    "reported for completeness, the kernel is latency/barrier bound here"}
+    line = None
+    if rank == 0:
+        sol0 = sols[-1]
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            seconds, inner, _ = cpu_oracle_sample(lp, args.tol, args.cpu_sample_outer)
+            full_inner = sol0.inner_iter
+            cpu = {"value": seconds / inner * full_inner, "unit": "s", "cores": blas_threads(),
+                   "kind": "port",
+                   "sample": (f"oracle (reference algorithm, SuperLU stand-in factor) on the first "
+                              f"{args.cpu_sample_outer} outer iterations = {inner} inner IPM iterations, "
+                              f"{seconds:.1f} s, scaled to the {full_inner} inner iterations of the "
+                              f"device solve")}
+        line = {
+            "metric": METRIC, "value": per_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * per_step, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "tol": args.tol, "l2": "256 MB L2 flush between steps",
+                       "outer_iterations": sol0.outer_iter, "inner_iterations": sol0.inner_iter,
+                       "objective": sol0.obj, "status": sol0.status,
+                       "pcg_iterations_per_step": pcg_its / args.steps},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "lp_per_s": world / per_step,
+        }
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    if dist:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, rank, world)
+        else:
+            line = run_ours(args, rank, world, local_rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

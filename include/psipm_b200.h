@@ -61,6 +61,9 @@ typedef struct {
     int32_t ok;              /* HSD variant: converged flag */
     double relative_residual;/* ||rhs - H x|| / max(1, ||rhs||) in FP64 */
     double seconds;          /* device time of the call (CUDA events) */
+    double phase_seconds[4]; /* device time by phase: [0] H·p passes, [1] vector
+                                updates, [2] preconditioner applies, [3] setup and
+                                true-residual checks (%globaltimer, block 0) */
 } psipm_pcg_info;
 
 typedef struct {
@@ -164,6 +167,11 @@ int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev,
                     double* dx_dev, double* dy_dev, psipm_pcg_info* info);
 
 /* ---- diagnostics ---------------------------------------------------------------- */
+/* Device-side stopwatch on the handle's stream (CUDA events): start records
+ * an event; stop records a second one, waits for it and returns the elapsed
+ * seconds.  Everything the handle launches in between is inside the interval. */
+int psipm_timer_start(psipm_handle* h);
+int psipm_timer_stop(psipm_handle* h, double* seconds);
 /* Kernels launched by this handle since creation (all of them are this
  * library's own kernels). */
 int64_t psipm_kernel_launches(const psipm_handle* h);

@@ -1,0 +1,1157 @@
+// C ABI of libpsipm_b200 (declared in include/psipm_b200.h).
+//
+// Each entry point validates its arguments, runs on the handle's stream,
+// synchronises before returning and converts any failure into a status code
+// (the message is kept for psipm_last_error).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels_factor.cuh"
+#include "kernels_pcg.cuh"
+#include "kernels_select.cuh"
+#include "symbolic.h"
+
+using namespace psipm;
+
+namespace {
+
+const double kShifts[8] = {0.0, 1e-14, 1e-12, 1e-10, 1e-8, 1e-6, 1e-4, 1e-2};
+// fronts with more rows than this are factored by the multi-CTA blocked path
+int kBigFront = 192;
+// supernodes with at least this many columns use the split triangular solve
+int kBigSolve = 96;
+
+// The two thresholds can be lowered through the environment
+// (PSIPM_BIG_FRONT, PSIPM_BIG_SOLVE) so that small test problems exercise
+// the large-front and split-solve code paths.
+void read_thresholds() {
+    if (const char* v = std::getenv("PSIPM_BIG_FRONT")) kBigFront = std::max(1, std::atoi(v));
+    if (const char* v = std::getenv("PSIPM_BIG_SOLVE")) kBigSolve = std::max(1, std::atoi(v));
+}
+constexpr int kRowsPerTask = 8;
+
+template <typename T>
+struct FactorStore {
+    DevBuf<T> ms, G, update, front, xp, yp, uvec, dscp, GT, fvec, bvec;
+};
+
+template <typename T>
+struct PcgStore {
+    DevBuf<T> rhs, x, r, z, p, q, t, tr, chunk_part, w, at_val, a_val;
+};
+
+}  // namespace
+
+struct psipm_handle {
+    int device = 0;
+    int precision = PSIPM_FP64;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tv0 = nullptr, tv1 = nullptr;
+    int64_t m = 0, n = 0, nnz = 0;
+    std::string err;
+    int64_t launches = 0;
+    int num_sms = 0;
+    int coop_blocks = 0;
+
+    // A in CSC on the host (needed by the symbolic analysis)
+    std::vector<int64_t> colptr;
+    std::vector<int32_t> rowidx;
+    std::vector<double> val;
+    std::vector<int64_t> cand;
+
+    // device matrix
+    DevBuf<int> at_ptr, at_idx, a_ptr, a_idx;
+    DevBuf<double> at_val, a_val;
+    DevBuf<int> short_rows, long_rows, long_chunk_ptr, chunk_beg, chunk_end;
+    int n_short = 0, n_long = 0, n_chunks = 0, vw = 32;
+    DevBuf<long long> d_cand;
+
+    // weights and scores
+    DevBuf<double> theta, w, diag_full, inv, scores;
+    double delta = 0.0;
+    bool have_theta = false;
+    bool scores_valid = false;
+
+    // core
+    std::vector<int64_t> core;
+    DevBuf<long long> d_core;
+    DevBuf<unsigned char> core_flags;  // candidate-local membership of the current core
+    bool core_dirty = true;            // core changed since the last symbolic analysis
+
+    // symbolic
+    Symbolic sym;
+    bool have_symbolic = false;
+    int n_symbolic = 0;
+    double symbolic_seconds = 0.0;
+    DevBuf<int> s_perm, s_iperm, s_first, s_rows, s_child_ptr, s_child_list, s_relind, s_level_sn;
+    DevBuf<int> s_ent_col, s_ent_rowpos, s_ent_row, s_ent_colg, s_contrib_col;
+    DevBuf<long long> s_rowptr, s_panel_off, s_update_off, s_uvec_off, s_entptr, s_ent_ptr,
+        s_diag_entry, s_fg_ptr, s_fg_idx, s_front_off;
+    DevBuf<double> s_contrib_val;
+    DevBuf<int> fwd_ptr_d, bwd_ptr_d;
+    DevBuf<int4> fwd_tasks_d, bwd_tasks_d;
+    std::vector<int> fwd_ptr, bwd_ptr, fpre_ptr, bpre_ptr;
+    DevBuf<int> fpre_ptr_d, bpre_ptr_d;
+    DevBuf<int4> fpre_tasks_d, bpre_tasks_d;
+    std::vector<int> solve_big_sn;        // supernodes with a transposed panel
+    std::vector<int64_t> gt_off_host;
+    DevBuf<long long> gt_off_d;
+    int64_t front_total = 0;
+    // per level: fronts factored one per CTA (small) and by the multi-CTA path (big)
+    std::vector<int> small_ptr, small_sn, big_ptr, big_sn;
+    std::vector<int64_t> front_off_host;
+    DevBuf<int> small_sn_d;
+
+    // numeric
+    DevBuf<double> pval, dscp64;
+    FactorStore<double> f64;
+    bool have_factor = false;
+    double factor_seconds = 0.0;
+    DevBuf<int> fail;
+
+    // PCG
+    PcgStore<double> p64;
+    DevBuf<double> part;
+    DevBuf<int> ctrl, iout;
+    DevBuf<double> dout, alphas, betas, history;
+    DevBuf<double> r1, r2, dx, dy, wr1;
+
+    // selection scratch
+    DevBuf<unsigned char> flag_a, flag_b, flag_c, mand_flags;
+    DevBuf<int> eq, eqscan;
+    DevBuf<unsigned int> hist;
+    DevBuf<unsigned long long> counter;
+};
+
+namespace {
+
+#define LAUNCH(h, ...)                \
+    do {                              \
+        __VA_ARGS__;                  \
+        PSIPM_CHECK_LAUNCH();         \
+        ++(h)->launches;              \
+    } while (0)
+
+int fail_code(psipm_handle* h, const Failure& f) {
+    if (h) h->err = f.what();
+    return f.code;
+}
+
+template <typename F>
+int guarded(psipm_handle* h, F&& body) {
+    if (!h) return PSIPM_ERR_ARGUMENT;
+    try {
+        PSIPM_CUDA(cudaSetDevice(h->device));
+        body();
+        PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+        return PSIPM_OK;
+    } catch (const Failure& f) {
+        return fail_code(h, f);
+    } catch (const std::bad_alloc&) {
+        h->err = "host allocation failed";
+        return PSIPM_ERR_MEMORY;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        return PSIPM_ERR_ARGUMENT;
+    }
+}
+
+inline int blocks_for(int64_t n, int threads) { return (int)std::max<int64_t>(1, (n + threads - 1) / threads); }
+
+void require(bool cond, int code, const char* msg) {
+    if (!cond) throw Failure(code, msg);
+}
+
+// ---------------------------------------------------------------------------
+// device layout of A
+void build_matrix(psipm_handle* h) {
+    const int64_t m = h->m, n = h->n, nnz = h->nnz;
+    // A^T CSR == A CSC
+    std::vector<int> at_ptr(n + 1);
+    for (int64_t j = 0; j <= n; ++j) at_ptr[j] = (int)h->colptr[j];
+    h->at_ptr.upload(at_ptr, h->stream);
+    h->at_idx.upload(h->rowidx.data(), nnz, h->stream);
+    h->at_val.upload(h->val.data(), nnz, h->stream);
+    // A CSR (column indices ascending within a row)
+    std::vector<int> a_ptr(m + 1, 0), a_idx(nnz);
+    std::vector<double> a_val(nnz);
+    for (int64_t k = 0; k < nnz; ++k) ++a_ptr[h->rowidx[k] + 1];
+    for (int64_t i = 0; i < m; ++i) a_ptr[i + 1] += a_ptr[i];
+    {
+        std::vector<int> f(a_ptr.begin(), a_ptr.end() - 1);
+        for (int64_t j = 0; j < n; ++j)
+            for (int64_t k = h->colptr[j]; k < h->colptr[j + 1]; ++k) {
+                int i = h->rowidx[k];
+                a_idx[f[i]] = (int)j;
+                a_val[f[i]] = h->val[k];
+                ++f[i];
+            }
+    }
+    h->a_ptr.upload(a_ptr, h->stream);
+    h->a_idx.upload(a_idx, h->stream);
+    h->a_val.upload(a_val, h->stream);
+    // short / long rows
+    std::vector<int> shortr, longr, lcp{0}, cb, ce;
+    int64_t short_nnz = 0, short_cnt = 0;
+    for (int64_t i = 0; i < m; ++i) {
+        int len = a_ptr[i + 1] - a_ptr[i];
+        if (len > kLongRow) {
+            longr.push_back((int)i);
+            for (int b = a_ptr[i]; b < a_ptr[i + 1]; b += kLongRow) {
+                cb.push_back(b);
+                ce.push_back(std::min(b + kLongRow, a_ptr[i + 1]));
+            }
+            lcp.push_back((int)cb.size());
+        } else {
+            shortr.push_back((int)i);
+            short_nnz += len;
+            ++short_cnt;
+        }
+    }
+    double avg = short_cnt ? (double)short_nnz / (double)short_cnt : 1.0;
+    int vw = 1;
+    while (vw < 32 && vw < avg) vw <<= 1;
+    h->vw = vw;
+    h->n_short = (int)shortr.size();
+    h->n_long = (int)longr.size();
+    h->n_chunks = (int)cb.size();
+    h->short_rows.upload(shortr, h->stream);
+    h->long_rows.upload(longr, h->stream);
+    h->long_chunk_ptr.upload(lcp, h->stream);
+    h->chunk_beg.upload(cb, h->stream);
+    h->chunk_end.upload(ce, h->stream);
+    // candidates: columns with at least two nonzeros
+    h->cand.clear();
+    for (int64_t j = 0; j < n; ++j)
+        if (h->colptr[j + 1] - h->colptr[j] >= 2) h->cand.push_back(j);
+    std::vector<long long> cl(h->cand.begin(), h->cand.end());
+    h->d_cand.upload(cl, h->stream);
+}
+
+template <typename T>
+SpmvLayout spmv_layout(psipm_handle* h) {
+    SpmvLayout s;
+    s.m = (int)h->m;
+    s.n = (int)h->n;
+    s.at_ptr = h->at_ptr.p;
+    s.at_idx = h->at_idx.p;
+    s.a_ptr = h->a_ptr.p;
+    s.a_idx = h->a_idx.p;
+    s.vw = h->vw;
+    s.short_rows = h->short_rows.p;
+    s.n_short = h->n_short;
+    s.long_rows = h->long_rows.p;
+    s.n_long = h->n_long;
+    s.long_chunk_ptr = h->long_chunk_ptr.p;
+    s.chunk_beg = h->chunk_beg.p;
+    s.chunk_end = h->chunk_end.p;
+    s.n_chunks = h->n_chunks;
+    return s;
+}
+
+PcgArgs<double> pcg_args(psipm_handle* h) {
+    PcgArgs<double> a;
+    a.sp = spmv_layout<double>(h);
+    a.at_val = h->at_val.p;
+    a.a_val = h->a_val.p;
+    a.w = h->w.p;
+    a.delta = h->delta;
+    PrecLayout<double>& pc = a.pc;
+    pc.m = (int)h->m;
+    if (h->have_symbolic) {
+        pc.perm = h->s_perm.p;
+        pc.iperm = h->s_iperm.p;
+        pc.dscp = h->f64.dscp.p;
+        pc.G = h->f64.G.p;
+        pc.panel_off = h->s_panel_off.p;
+        pc.sn_first = h->s_first.p;
+        pc.sn_rowptr = h->s_rowptr.p;
+        pc.sn_rows = h->s_rows.p;
+        pc.uvec_off = h->s_uvec_off.p;
+        pc.fg_ptr = h->s_fg_ptr.p;
+        pc.fg_idx = h->s_fg_idx.p;
+        pc.nlevels = h->sym.nlevels;
+        pc.fwd_ptr = h->fwd_ptr_d.p;
+        pc.fwd_tasks = h->fwd_tasks_d.p;
+        pc.bwd_ptr = h->bwd_ptr_d.p;
+        pc.bwd_tasks = h->bwd_tasks_d.p;
+        pc.xp = h->f64.xp.p;
+        pc.yp = h->f64.yp.p;
+        pc.uvec = h->f64.uvec.p;
+        pc.fpre_ptr = h->fpre_ptr_d.p;
+        pc.fpre_tasks = h->fpre_tasks_d.p;
+        pc.bpre_ptr = h->bpre_ptr_d.p;
+        pc.bpre_tasks = h->bpre_tasks_d.p;
+        pc.fvec = h->f64.fvec.p;
+        pc.bvec = h->f64.bvec.p;
+        pc.GT = h->f64.GT.p;
+        pc.gt_off = h->gt_off_d.p;
+    }
+    PcgStore<double>& st = h->p64;
+    const int64_t m = h->m, n = h->n;
+    st.x.reserve(m);
+    st.r.reserve(m);
+    st.z.reserve(m);
+    st.p.reserve(m);
+    st.q.reserve(m);
+    st.t.reserve(n);
+    st.tr.reserve(m);
+    st.chunk_part.reserve(std::max(1, h->n_chunks));
+    h->part.reserve((size_t)2 * 4 * std::max(1, h->coop_blocks));
+    h->ctrl.reserve(4);
+    h->iout.reserve(16);
+    h->dout.reserve(8);
+    a.x = st.x.p;
+    a.r = st.r.p;
+    a.z = st.z.p;
+    a.p = st.p.p;
+    a.q = st.q.p;
+    a.t = st.t.p;
+    a.tr = st.tr.p;
+    a.chunk_part = st.chunk_part.p;
+    a.part = h->part.p;
+    a.ctrl = h->ctrl.p;
+    a.iout = h->iout.p;
+    a.dout = h->dout.p;
+    return a;
+}
+
+size_t pcg_smem() { return (size_t)kPcgWarps * kStageChunk * sizeof(double); }
+
+void launch_coop(psipm_handle* h, const void* fn, void** args) {
+    dim3 grid(h->coop_blocks), block(kPcgThreads);
+    PSIPM_CUDA(cudaLaunchCooperativeKernel(fn, grid, block, args, pcg_smem(), h->stream));
+    ++h->launches;
+}
+
+// ---------------------------------------------------------------------------
+// symbolic analysis of the current core and upload of its arrays
+void analyse(psipm_handle* h) {
+    auto t0 = std::chrono::steady_clock::now();
+    read_thresholds();
+    SymbolicOptions opt;
+    Symbolic S;
+    std::vector<int64_t> core(h->core.begin(), h->core.end());
+    int rc = build_symbolic((int32_t)h->m, h->n, h->colptr.data(), h->rowidx.data(), h->val.data(),
+                            core.data(), (int64_t)core.size(), opt, S);
+    if (rc != 0) throw Failure(PSIPM_ERR_SYMBOLIC, "symbolic analysis failed with code " + std::to_string(rc));
+    h->sym = std::move(S);
+    Symbolic& s = h->sym;
+    cudaStream_t st = h->stream;
+    h->s_perm.upload(s.perm, st);
+    h->s_iperm.upload(s.iperm, st);
+    h->s_first.upload(s.sn_first, st);
+    h->s_rows.upload(s.sn_rows, st);
+    h->s_child_ptr.upload(s.child_ptr, st);
+    h->s_child_list.upload(s.child_list, st);
+    h->s_relind.upload(s.relind, st);
+    h->s_level_sn.upload(s.level_sn, st);
+    h->s_ent_col.upload(s.ent_col, st);
+    h->s_ent_rowpos.upload(s.ent_rowpos, st);
+    h->s_contrib_col.upload(s.contrib_col, st);
+    h->s_contrib_val.upload(s.contrib_val, st);
+    auto up64 = [&](DevBuf<long long>& d, const std::vector<int64_t>& v) {
+        std::vector<long long> t(v.begin(), v.end());
+        d.upload(t, st);
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+    };
+    up64(h->s_rowptr, s.sn_rowptr);
+    up64(h->s_panel_off, s.panel_off);
+    up64(h->s_update_off, s.update_off);
+    up64(h->s_uvec_off, s.uvec_off);
+    up64(h->s_entptr, s.sn_entptr);
+    up64(h->s_ent_ptr, s.ent_ptr);
+    up64(h->s_diag_entry, s.diag_entry);
+    up64(h->s_fg_ptr, s.fgather_ptr);
+    up64(h->s_fg_idx, s.fgather_idx);
+    // entry row/col in permuted numbering (for the Jacobi scaling)
+    std::vector<int> er(s.nentries), ec(s.nentries);
+    for (int64_t e = 0; e < s.nentries; ++e) {
+        int sn = s.ent_sn[e];
+        ec[e] = s.sn_first[sn] + s.ent_col[e];
+        er[e] = s.sn_rows[s.sn_rowptr[sn] + s.ent_rowpos[e]];
+    }
+    h->s_ent_row.upload(er, st);
+    h->s_ent_colg.upload(ec, st);
+    // front workspace offsets per level
+    std::vector<int64_t> foff(s.ns, 0);
+    int64_t fmax_total = 0;
+    for (int l = 0; l < s.nlevels; ++l) {
+        int64_t off = 0;
+        for (int q = s.level_ptr[l]; q < s.level_ptr[l + 1]; ++q) {
+            int sn = s.level_sn[q];
+            int64_t r = s.sn_rowptr[sn + 1] - s.sn_rowptr[sn];
+            foff[sn] = off;
+            off += r * r;
+        }
+        fmax_total = std::max(fmax_total, off);
+    }
+    h->front_total = fmax_total;
+    h->front_off_host = foff;
+    up64(h->s_front_off, foff);
+    // triangular-solve tasks per level.  Small supernodes: one warp per 32
+    // rows (forward) / 32 columns (backward), front vector staged in shared
+    // memory.  Big supernodes (c >= kBigSolve): a pre-phase assembles the
+    // vectors in global memory, then warps take kRowsPerTask rows each.
+    std::vector<int4> ft, bt, fp, bp;
+    h->fwd_ptr.assign(s.nlevels + 1, 0);
+    h->bwd_ptr.assign(s.nlevels + 1, 0);
+    h->fpre_ptr.assign(s.nlevels + 1, 0);
+    h->bpre_ptr.assign(s.nlevels + 1, 0);
+    h->solve_big_sn.clear();
+    h->gt_off_host.assign(s.ns + 1, 0);
+    int64_t gt_total = 0;
+    for (int l = 0; l < s.nlevels; ++l) {
+        for (int q = s.level_ptr[l]; q < s.level_ptr[l + 1]; ++q) {
+            int sn = s.level_sn[q];
+            int c = s.sn_first[sn + 1] - s.sn_first[sn];
+            int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
+            if (c >= kBigSolve) {
+                h->solve_big_sn.push_back(sn);
+                h->gt_off_host[sn] = gt_total;
+                gt_total += (int64_t)r * c;
+                for (int p0 = 0; p0 < r; p0 += 32) {
+                    fp.push_back(make_int4(sn, p0, std::min(r, p0 + 32), 0));
+                    bp.push_back(make_int4(sn, p0, std::min(r, p0 + 32), 0));
+                }
+                for (int r0 = 0; r0 < r; r0 += kRowsPerTask)
+                    ft.push_back(make_int4(sn, r0, std::min(r, r0 + kRowsPerTask), 2));
+                for (int j0 = 0; j0 < c; j0 += kRowsPerTask)
+                    bt.push_back(make_int4(sn, j0, std::min(c, j0 + kRowsPerTask), 2));
+            } else {
+                for (int r0 = 0; r0 < r; r0 += 32) ft.push_back(make_int4(sn, r0, std::min(r, r0 + 32), 0));
+                for (int j0 = 0; j0 < c; j0 += 32) bt.push_back(make_int4(sn, j0, std::min(c, j0 + 32), 0));
+            }
+        }
+        h->fwd_ptr[l + 1] = (int)ft.size();
+        h->bwd_ptr[l + 1] = (int)bt.size();
+        h->fpre_ptr[l + 1] = (int)fp.size();
+        h->bpre_ptr[l + 1] = (int)bp.size();
+    }
+    h->fpre_ptr_d.upload(h->fpre_ptr, st);
+    h->bpre_ptr_d.upload(h->bpre_ptr, st);
+    h->fpre_tasks_d.upload(fp, st);
+    h->bpre_tasks_d.upload(bp, st);
+    {
+        std::vector<long long> go(h->gt_off_host.begin(), h->gt_off_host.end());
+        h->gt_off_d.upload(go, st);
+    }
+    h->f64.GT.reserve(std::max<int64_t>(1, gt_total));
+    h->f64.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
+    h->f64.bvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
+    h->small_ptr.assign(s.nlevels + 1, 0);
+    h->big_ptr.assign(s.nlevels + 1, 0);
+    h->small_sn.clear();
+    h->big_sn.clear();
+    for (int l = 0; l < s.nlevels; ++l) {
+        for (int q = s.level_ptr[l]; q < s.level_ptr[l + 1]; ++q) {
+            int sn = s.level_sn[q];
+            int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
+            if (r > kBigFront)
+                h->big_sn.push_back(sn);
+            else
+                h->small_sn.push_back(sn);
+        }
+        h->small_ptr[l + 1] = (int)h->small_sn.size();
+        h->big_ptr[l + 1] = (int)h->big_sn.size();
+    }
+    h->small_sn_d.upload(h->small_sn, st);
+    h->fwd_ptr_d.upload(h->fwd_ptr, st);
+    h->bwd_ptr_d.upload(h->bwd_ptr, st);
+    h->fwd_tasks_d.upload(ft, st);
+    h->bwd_tasks_d.upload(bt, st);
+    // numeric storage
+    h->pval.reserve(std::max<int64_t>(1, s.nentries));
+    h->f64.ms.reserve(std::max<int64_t>(1, s.nentries));
+    h->f64.G.reserve(std::max<int64_t>(1, s.panel_total));
+    h->f64.update.reserve(std::max<int64_t>(1, s.update_total));
+    h->f64.front.reserve(std::max<int64_t>(1, fmax_total));
+    h->f64.xp.reserve(h->m);
+    h->f64.yp.reserve(h->m);
+    h->f64.uvec.reserve(std::max<int64_t>(1, s.uvec_total));
+    h->f64.dscp.reserve(h->m);
+    h->fail.reserve(1);
+    PSIPM_CUDA(cudaStreamSynchronize(st));
+    h->have_symbolic = true;
+    h->have_factor = false;
+    h->core_dirty = false;
+    ++h->n_symbolic;
+    h->symbolic_seconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void compute_weights(psipm_handle* h) {
+    const int64_t n = h->n, m = h->m;
+    h->w.reserve(n);
+    h->diag_full.reserve(m);
+    LAUNCH(h, k_weights<<<blocks_for(n, 256), 256, 0, h->stream>>>(n, h->theta.p, h->w.p));
+    LAUNCH(h, k_diag_full<<<blocks_for(m, 256), 256, 0, h->stream>>>(
+                  (int)m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->w.p, h->diag_full.p));
+}
+
+
+// one large front by the multi-CTA blocked path (kernels_factor.cuh)
+template <typename T>
+void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
+    const Symbolic& s = h->sym;
+    cudaStream_t st = h->stream;
+    const int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
+    const int c = s.sn_first[sn + 1] - s.sn_first[sn];
+    // front offsets live on the device; the host keeps its own copy
+    T* F = fa.front + h->front_off_host[sn];
+    PSIPM_CUDA(cudaMemsetAsync(F, 0, (size_t)r * r * sizeof(T), st));
+    const long long e0 = s.sn_entptr[sn], e1 = s.sn_entptr[sn + 1];
+    if (e1 > e0)
+        LAUNCH(h, k_front_scatter<T><<<std::min(blocks_for(e1 - e0, 256), 4096), 256, 0, st>>>(
+                      F, r, e0, e1, fa.ent_col, fa.ent_rowpos, fa.ms, fa.eta));
+    for (int ci = s.child_ptr[sn]; ci < s.child_ptr[sn + 1]; ++ci) {
+        const int ch = s.child_list[ci];
+        const int rc = (int)(s.uvec_off[ch + 1] - s.uvec_off[ch]);
+        if (rc <= 0) continue;
+        const long long n2 = (long long)rc * rc;
+        LAUNCH(h, k_front_extend_add<T><<<std::min(blocks_for(n2, 256), 8192), 256, 0, st>>>(
+                      F, r, fa.update + s.update_off[ch], rc, fa.relind + s.uvec_off[ch]));
+    }
+    const size_t trsm_smem = 2 * kNB * (kNB + 1) * sizeof(T);
+    const size_t syrk_smem = 2 * kNB * (kNB + 1) * sizeof(T);
+    for (int k0 = 0; k0 < c; k0 += kNB) {
+        const int kb = std::min(kNB, c - k0);
+        LAUNCH(h, k_potrf_diag<T><<<1, 256, 0, st>>>(F, r, k0, kb, fa.fail));
+        const int rows = r - k0 - kb;
+        if (rows <= 0) continue;
+        LAUNCH(h, k_trsm_panel<T><<<blocks_for(rows, kTrsmRows), kTrsmRows, trsm_smem, st>>>(F, r, k0, kb));
+        const int ntile = (rows + 63) / 64;
+        LAUNCH(h, k_syrk_update<T><<<ntile * (ntile + 1) / 2, 256, syrk_smem, st>>>(F, r, k0, kb, ntile));
+    }
+    if (r > c) {
+        const long long n2 = (long long)(r - c) * (r - c);
+        LAUNCH(h, k_extract_update<T><<<std::min(blocks_for(n2, 256), 8192), 256, 0, st>>>(
+                      F, r, c, fa.update + s.update_off[sn]));
+    }
+    LAUNCH(h, k_g_trsm<T><<<blocks_for(r, 32), 256, 0, st>>>(F, r, c, fa.G + s.panel_off[sn]));
+}
+
+// ---------------------------------------------------------------------------
+// radix top-k among eligible entries; sets out_flag[i] = 1 for the selected
+void select_top(psipm_handle* h, const double* score, const unsigned char* mask, int64_t nsc,
+                int64_t count, unsigned char* out_flag) {
+    if (count <= 0 || nsc == 0) return;
+    cudaStream_t st = h->stream;
+    h->counter.reserve(1);
+    PSIPM_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(unsigned long long), st));
+    const int gb = std::min(blocks_for(nsc, kSelectThreads), 4 * std::max(1, h->num_sms));
+    LAUNCH(h, k_count_eligible<<<gb, kSelectThreads, 0, st>>>(nsc, score, mask, h->counter.p));
+    unsigned long long nel = 0;
+    PSIPM_CUDA(cudaMemcpyAsync(&nel, h->counter.p, sizeof(nel), cudaMemcpyDeviceToHost, st));
+    PSIPM_CUDA(cudaStreamSynchronize(st));
+    h->eq.reserve(nsc);
+    h->eqscan.reserve(nsc);
+    if ((int64_t)nel <= count) {
+        LAUNCH(h, k_mark_threshold<<<blocks_for(nsc, 256), 256, 0, st>>>(nsc, score, mask, 0ull, 1,
+                                                                          out_flag, h->eq.p));
+        return;
+    }
+    unsigned long long prefix = 0, pmask = 0;
+    int64_t need = count;
+    h->hist.reserve(256);
+    std::vector<unsigned int> hh(256);
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        PSIPM_CUDA(cudaMemsetAsync(h->hist.p, 0, 256 * sizeof(unsigned int), st));
+        LAUNCH(h, k_radix_hist<<<gb, kSelectThreads, 0, st>>>(nsc, score, mask, shift, prefix, pmask,
+                                                               h->hist.p));
+        PSIPM_CUDA(cudaMemcpyAsync(hh.data(), h->hist.p, 256 * sizeof(unsigned int),
+                                   cudaMemcpyDeviceToHost, st));
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        int64_t cum = 0;
+        int b = 255;
+        for (; b >= 0; --b) {
+            if (cum + (int64_t)hh[b] >= need) break;
+            cum += hh[b];
+        }
+        if (b < 0) throw Failure(PSIPM_ERR_BOUNDS, "radix select lost track of the threshold");
+        need -= cum;
+        prefix |= (unsigned long long)b << shift;
+        pmask |= 0xffull << shift;
+    }
+    // keys > prefix selected; first `need` equal keys by index
+    LAUNCH(h, k_mark_threshold<<<blocks_for(nsc, 256), 256, 0, st>>>(nsc, score, mask, prefix, 0,
+                                                                      out_flag, h->eq.p));
+    // exclusive scan of eq on the host (ties are rare and the array is modest)
+    std::vector<int> eqh(nsc);
+    PSIPM_CUDA(cudaMemcpyAsync(eqh.data(), h->eq.p, nsc * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PSIPM_CUDA(cudaStreamSynchronize(st));
+    int acc = 0;
+    for (int64_t i = 0; i < nsc; ++i) {
+        int v = eqh[i];
+        eqh[i] = acc;
+        acc += v;
+    }
+    h->eqscan.upload(eqh, st);
+    LAUNCH(h, k_mark_ties<<<blocks_for(nsc, 256), 256, 0, st>>>(nsc, h->eq.p, h->eqscan.p, need, out_flag));
+}
+
+int64_t count_flags(psipm_handle* h, const unsigned char* flags, int64_t n) {
+    std::vector<unsigned char> f(n);
+    if (n) PSIPM_CUDA(cudaMemcpyAsync(f.data(), flags, n, cudaMemcpyDeviceToHost, h->stream));
+    PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+    int64_t c = 0;
+    for (auto v : f) c += v;
+    return c;
+}
+
+std::vector<unsigned char> download_flags(psipm_handle* h, const unsigned char* flags, int64_t n) {
+    std::vector<unsigned char> f(n);
+    if (n) PSIPM_CUDA(cudaMemcpyAsync(f.data(), flags, n, cudaMemcpyDeviceToHost, h->stream));
+    PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+    return f;
+}
+
+void set_core_internal(psipm_handle* h, std::vector<int64_t> newcore) {
+    if (newcore != h->core) {
+        h->core = std::move(newcore);
+        h->core_dirty = true;
+    }
+    std::vector<long long> c(h->core.begin(), h->core.end());
+    h->d_core.upload(c, h->stream);
+    // candidate-local flags
+    const int64_t nc = (int64_t)h->cand.size();
+    std::vector<unsigned char> f(nc, 0);
+    for (int64_t g : h->core) {
+        auto it = std::lower_bound(h->cand.begin(), h->cand.end(), g);
+        if (it != h->cand.end() && *it == g) f[it - h->cand.begin()] = 1;
+    }
+    h->core_flags.upload(f, h->stream);
+}
+
+void run_pcg(psipm_handle* h, const double* rhs_dev, double tol, int maxit, int variant, int replacement,
+             double gap_tol, psipm_pcg_info* info) {
+    require(h->have_factor, PSIPM_ERR_STATE, "pcg before a successful factor");
+    PcgArgs<double> a = pcg_args(h);
+    a.rhs = rhs_dev;
+    a.variant = variant;
+    a.maxit = maxit;
+    a.replacement = replacement;
+    a.tol = tol;
+    a.gap_tol = gap_tol;
+    h->alphas.reserve(std::max(1, maxit));
+    h->betas.reserve(std::max(1, maxit));
+    h->history.reserve(maxit + 2);
+    a.alphas = h->alphas.p;
+    a.betas = h->betas.p;
+    a.history = h->history.p;
+    PSIPM_CUDA(cudaMemsetAsync(h->ctrl.p, 0, 4 * sizeof(int), h->stream));
+    void* args[] = {&a};
+    PSIPM_CUDA(cudaEventRecord(h->ev0, h->stream));
+    launch_coop(h, (const void*)k_pcg<double>, args);
+    PSIPM_CUDA(cudaEventRecord(h->ev1, h->stream));
+    int io[16];
+    double dd[8];
+    PSIPM_CUDA(cudaMemcpyAsync(io, h->iout.p, 9 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    PSIPM_CUDA(cudaMemcpyAsync(dd, h->dout.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    PSIPM_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->info = io[0];
+        info->iterations = io[1];
+        info->matvecs = io[2];
+        info->replacements = io[3];
+        info->residual_checks = io[4];
+        info->n_alpha = io[5];
+        info->n_beta = io[6];
+        info->n_history = io[7];
+        info->ok = io[8];
+        info->relative_residual = dd[0];
+        info->seconds = ms * 1e-3;
+        for (int q = 0; q < 4; ++q) info->phase_seconds[q] = dd[2 + q];
+    }
+}
+
+void copy_out(psipm_handle* h, double* host, const double* dev, int64_t n) {
+    if (host && n) PSIPM_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const int32_t* rowidx,
+                 const double* values, int32_t device, int32_t precision, psipm_handle** out) {
+    if (!out || m <= 0 || n < 0 || nnz < 0 || !colptr || (nnz && (!rowidx || !values)))
+        return PSIPM_ERR_ARGUMENT;
+    if (m >= (1ll << 31) || n >= (1ll << 31) || nnz >= (1ll << 31)) return PSIPM_ERR_UNSUPPORTED;
+    if (precision != PSIPM_FP64 && precision != PSIPM_FP32_REFINED) return PSIPM_ERR_ARGUMENT;
+    *out = nullptr;
+    if (colptr[0] != 0 || colptr[n] != nnz) return PSIPM_ERR_ARGUMENT;
+    for (int64_t j = 0; j < n; ++j) {
+        if (colptr[j + 1] < colptr[j]) return PSIPM_ERR_ARGUMENT;
+        for (int64_t k = colptr[j]; k < colptr[j + 1]; ++k) {
+            if (rowidx[k] < 0 || rowidx[k] >= m) return PSIPM_ERR_ARGUMENT;
+            if (k > colptr[j] && rowidx[k] <= rowidx[k - 1]) return PSIPM_ERR_ARGUMENT;
+        }
+    }
+    std::unique_ptr<psipm_handle> h(new psipm_handle());
+    h->device = device;
+    h->precision = precision;
+    h->m = m;
+    h->n = n;
+    h->nnz = nnz;
+    h->colptr.assign(colptr, colptr + n + 1);
+    h->rowidx.assign(rowidx, rowidx + nnz);
+    h->val.assign(values, values + nnz);
+    int rc = guarded(h.get(), [&]() {
+        int ndev = 0;
+        PSIPM_CUDA(cudaGetDeviceCount(&ndev));
+        require(device >= 0 && device < ndev, PSIPM_ERR_ARGUMENT, "no such CUDA device");
+        PSIPM_CUDA(cudaSetDevice(device));
+        PSIPM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        PSIPM_CUDA(cudaEventCreate(&h->ev0));
+        PSIPM_CUDA(cudaEventCreate(&h->ev1));
+        PSIPM_CUDA(cudaEventCreate(&h->tv0));
+        PSIPM_CUDA(cudaEventCreate(&h->tv1));
+        cudaDeviceProp prop;
+        PSIPM_CUDA(cudaGetDeviceProperties(&prop, device));
+        h->num_sms = prop.multiProcessorCount;
+        require(prop.cooperativeLaunch, PSIPM_ERR_UNSUPPORTED, "device lacks cooperative launch");
+        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)pcg_smem()));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)pcg_smem()));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_trsm_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kNB * (kNB + 1) * sizeof(double))));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kNB * (kNB + 1) * sizeof(double))));
+        int per_sm = 0;
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double>, kPcgThreads,
+                                                                 pcg_smem()));
+        int per_sm2 = 0;
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_apply<double>, kPcgThreads,
+                                                                 pcg_smem()));
+        int per_sm3 = 0;
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_matvec<double>, kPcgThreads, 0));
+        per_sm = std::min(std::min(per_sm, per_sm2), per_sm3);
+        require(per_sm >= 1, PSIPM_ERR_UNSUPPORTED, "PCG kernel does not fit on an SM");
+        h->coop_blocks = std::min(per_sm, 2) * h->num_sms;
+        build_matrix(h.get());
+    });
+    if (rc != PSIPM_OK) {
+        std::string msg = h->err;
+        // keep the handle so the caller can read the message
+        *out = h.release();
+        return rc;
+    }
+    *out = h.release();
+    return PSIPM_OK;
+}
+
+void psipm_destroy(psipm_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->tv0) cudaEventDestroy(h->tv0);
+    if (h->tv1) cudaEventDestroy(h->tv1);
+    cudaStream_t s = h->stream;
+    delete h;
+    if (s) cudaStreamDestroy(s);
+}
+
+const char* psipm_last_error(const psipm_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int64_t psipm_num_candidates(const psipm_handle* h) { return h ? (int64_t)h->cand.size() : -1; }
+
+int psipm_get_candidates(const psipm_handle* h, int64_t* out) {
+    if (!h || !out) return PSIPM_ERR_ARGUMENT;
+    std::copy(h->cand.begin(), h->cand.end(), out);
+    return PSIPM_OK;
+}
+
+int psipm_set_theta(psipm_handle* h, const double* theta, double delta) {
+    if (!theta) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        h->theta.upload(theta, h->n, h->stream);
+        h->delta = delta;
+        compute_weights(h);
+        h->have_theta = true;
+        h->scores_valid = false;
+    });
+}
+
+int psipm_scores(psipm_handle* h, double fill_weight, double* scores, double* diagonal) {
+    return guarded(h, [&]() {
+        require(h->have_theta, PSIPM_ERR_STATE, "scores before set_theta");
+        const int64_t m = h->m, nc = (int64_t)h->cand.size();
+        const double tiny = 2.2250738585072014e-308;
+        h->inv.reserve(m);
+        h->scores.reserve(std::max<int64_t>(1, nc));
+        LAUNCH(h, k_inv_diag<<<blocks_for(m, 256), 256, 0, h->stream>>>((int)m, h->diag_full.p,
+                                                                        std::max(h->delta, tiny), h->inv.p));
+        if (nc)
+            LAUNCH(h, k_scores<<<blocks_for(nc, 256), 256, 0, h->stream>>>(
+                          nc, h->d_cand.p, h->at_ptr.p, h->at_idx.p, h->at_val.p, h->w.p, h->inv.p,
+                          fill_weight, h->scores.p));
+        h->scores_valid = true;
+        copy_out(h, scores, h->scores.p, nc);
+        copy_out(h, diagonal, h->diag_full.p, m);
+    });
+}
+
+int psipm_top_k(psipm_handle* h, const double* scores, int64_t nscores, const uint8_t* mask, int64_t count,
+                int64_t* out, int64_t* nout) {
+    if (!scores || nscores < 0 || !out || !nout) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        DevBuf<double> sc;
+        DevBuf<unsigned char> mk, fl;
+        sc.upload(scores, nscores, h->stream);
+        if (mask) mk.upload(mask, nscores, h->stream);
+        fl.zero(std::max<int64_t>(1, nscores), h->stream);
+        select_top(h, sc.p, mask ? mk.p : nullptr, nscores, count, fl.p);
+        auto f = download_flags(h, fl.p, nscores);
+        int64_t k = 0;
+        for (int64_t i = 0; i < nscores; ++i)
+            if (f[i]) out[k++] = i;
+        *nout = k;
+    });
+}
+
+int psipm_refresh_core(psipm_handle* h, int64_t target, double retention, int32_t stable,
+                       const int64_t* mandatory_local, int64_t nmandatory, int64_t* core_out, int64_t* ncore,
+                       double* retained) {
+    if (nmandatory < 0 || (nmandatory && !mandatory_local) || !core_out || !ncore) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->scores_valid, PSIPM_ERR_STATE, "refresh before scores");
+        cudaStream_t st = h->stream;
+        const int64_t nc = (int64_t)h->cand.size();
+        target = std::min(target, nc);
+        for (int64_t q = 0; q < nmandatory; ++q)
+            require(mandatory_local[q] >= 0 && mandatory_local[q] < nc && (q == 0 || mandatory_local[q] > mandatory_local[q - 1]),
+                    PSIPM_ERR_ARGUMENT, "mandatory positions must be sorted candidate-local indices");
+        const int64_t nn = std::max<int64_t>(1, nc);
+        h->flag_a.zero(nn, st);  // fixed
+        h->flag_b.zero(nn, st);  // scratch selection
+        h->flag_c.zero(nn, st);  // mask
+        h->mand_flags.zero(nn, st);
+        DevBuf<long long> mand;
+        {
+            std::vector<long long> mv(mandatory_local, mandatory_local + nmandatory);
+            mand.upload(mv, st);
+        }
+        if (nmandatory) {
+            LAUNCH(h, k_set_flags<<<blocks_for(nmandatory, 256), 256, 0, st>>>(nmandatory, mand.p, 1, h->flag_a.p));
+            LAUNCH(h, k_set_flags<<<blocks_for(nmandatory, 256), 256, 0, st>>>(nmandatory, mand.p, 1, h->mand_flags.p));
+        }
+        const int64_t old_size = (int64_t)h->core.size();
+        bool have_old = old_size > 0 && h->core_flags.p && h->core_flags.n >= (size_t)nc;
+        if (stable && have_old && target) {
+            int64_t keep = std::min<int64_t>(old_size, std::max<int64_t>(0, (int64_t)std::floor(retention * (double)target)));
+            if (keep) {
+                select_top(h, h->scores.p, h->core_flags.p, nc, keep, h->flag_b.p);
+                LAUNCH(h, k_flag_op<<<blocks_for(nc, 256), 256, 0, st>>>(nc, h->flag_a.p, h->flag_b.p, 1, h->flag_a.p));
+            }
+        }
+        int64_t nfixed = count_flags(h, h->flag_a.p, nc);
+        if (nfixed > target) {
+            if (nmandatory >= target) {
+                PSIPM_CUDA(cudaMemsetAsync(h->flag_a.p, 0, nc, st));
+                if (target)
+                    LAUNCH(h, k_set_flags<<<blocks_for(target, 256), 256, 0, st>>>(target, mand.p, 1, h->flag_a.p));
+            } else {
+                // optional = fixed & ~mandatory; keep the best (target - |mandatory|)
+                LAUNCH(h, k_flag_op<<<blocks_for(nc, 256), 256, 0, st>>>(nc, h->flag_a.p, h->mand_flags.p, 0, h->flag_c.p));
+                PSIPM_CUDA(cudaMemsetAsync(h->flag_b.p, 0, nc, st));
+                select_top(h, h->scores.p, h->flag_c.p, nc, target - nmandatory, h->flag_b.p);
+                LAUNCH(h, k_flag_op<<<blocks_for(nc, 256), 256, 0, st>>>(nc, h->mand_flags.p, h->flag_b.p, 1, h->flag_a.p));
+            }
+            nfixed = count_flags(h, h->flag_a.p, nc);
+        }
+        const int64_t remaining = target - nfixed;
+        if (remaining > 0) {
+            // available = ~fixed (fixed scores count as -inf, i.e. not eligible)
+            std::vector<unsigned char> fa = download_flags(h, h->flag_a.p, nc);
+            for (auto& v : fa) v = !v;
+            h->flag_c.upload(fa, st);
+            PSIPM_CUDA(cudaMemsetAsync(h->flag_b.p, 0, nc, st));
+            select_top(h, h->scores.p, h->flag_c.p, nc, remaining, h->flag_b.p);
+            LAUNCH(h, k_flag_op<<<blocks_for(nc, 256), 256, 0, st>>>(nc, h->flag_a.p, h->flag_b.p, 1, h->flag_a.p));
+        }
+        std::vector<unsigned char> nf = download_flags(h, h->flag_a.p, nc);
+        std::vector<unsigned char> of = have_old ? download_flags(h, h->core_flags.p, nc)
+                                                 : std::vector<unsigned char>(nc, 0);
+        std::vector<int64_t> newcore;
+        int64_t inter = 0;
+        for (int64_t i = 0; i < nc; ++i) {
+            if (nf[i]) newcore.push_back(h->cand[i]);
+            if (nf[i] && of[i]) ++inter;
+        }
+        if (retained) *retained = old_size ? (double)inter / (double)std::max<int64_t>(1, old_size) : 1.0;
+        std::copy(newcore.begin(), newcore.end(), core_out);
+        *ncore = (int64_t)newcore.size();
+        set_core_internal(h, std::move(newcore));
+    });
+}
+
+int psipm_set_core(psipm_handle* h, const int64_t* core, int64_t ncore) {
+    if (ncore < 0 || (ncore && !core)) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        std::vector<int64_t> c(core, core + ncore);
+        for (int64_t q = 0; q < ncore; ++q)
+            require(c[q] >= 0 && c[q] < h->n && (q == 0 || c[q] > c[q - 1]), PSIPM_ERR_ARGUMENT,
+                    "core must hold sorted, distinct column indices");
+        set_core_internal(h, std::move(c));
+    });
+}
+
+int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* shift_index,
+                 psipm_factor_info* info) {
+    if (start_shift < 0 || start_shift > 7) return PSIPM_ERR_ARGUMENT;
+    int status = guarded(h, [&]() {
+        require(h->have_theta, PSIPM_ERR_STATE, "factor before set_theta");
+        if (h->core_dirty || !h->have_symbolic) analyse(h);
+        h->delta = delta;
+        Symbolic& s = h->sym;
+        cudaStream_t st = h->stream;
+        PSIPM_CUDA(cudaEventRecord(h->ev0, st));
+        if (s.nentries)
+            LAUNCH(h, k_assemble_entries<<<blocks_for(s.nentries, 256), 256, 0, st>>>(
+                          s.nentries, h->s_ent_ptr.p, h->s_contrib_col.p, h->s_contrib_val.p, h->d_core.p,
+                          h->w.p, h->pval.p));
+        LAUNCH(h, k_diag_fix<<<blocks_for(h->m, 256), 256, 0, st>>>((int)h->m, h->s_diag_entry.p, h->s_perm.p,
+                                                                     h->diag_full.p, delta, h->pval.p,
+                                                                     h->f64.dscp.p));
+        if (s.nentries)
+            LAUNCH(h, k_scale_entries<double><<<blocks_for(s.nentries, 256), 256, 0, st>>>(
+                          s.nentries, h->s_ent_row.p, h->s_ent_colg.p, h->pval.p, h->f64.dscp.p, h->f64.ms.p));
+        FactorArgs<double> fa;
+        fa.sn_first = h->s_first.p;
+        fa.sn_rowptr = h->s_rowptr.p;
+        fa.panel_off = h->s_panel_off.p;
+        fa.update_off = h->s_update_off.p;
+        fa.uvec_off = h->s_uvec_off.p;
+        fa.child_ptr = h->s_child_ptr.p;
+        fa.child_list = h->s_child_list.p;
+        fa.relind = h->s_relind.p;
+        fa.sn_entptr = h->s_entptr.p;
+        fa.ent_col = h->s_ent_col.p;
+        fa.ent_rowpos = h->s_ent_rowpos.p;
+        fa.ms = h->f64.ms.p;
+        fa.G = h->f64.G.p;
+        fa.update = h->f64.update.p;
+        fa.front = h->f64.front.p;
+        fa.front_off = h->s_front_off.p;
+        fa.fail = h->fail.p;
+        int used = -1;
+        for (int k = start_shift; k < 8; ++k) {
+            fa.eta = kShifts[k];
+            PSIPM_CUDA(cudaMemsetAsync(h->fail.p, 0, sizeof(int), st));
+            for (int l = 0; l < s.nlevels; ++l) {
+                int cnt = h->small_ptr[l + 1] - h->small_ptr[l];
+                if (cnt)
+                    LAUNCH(h, k_factor_level<double><<<cnt, kFactorThreads, 0, st>>>(fa, h->small_sn_d.p + h->small_ptr[l]));
+                for (int q = h->big_ptr[l]; q < h->big_ptr[l + 1]; ++q) factor_big_front<double>(h, h->big_sn[q], fa);
+            }
+            int failed = 0;
+            PSIPM_CUDA(cudaMemcpyAsync(&failed, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PSIPM_CUDA(cudaStreamSynchronize(st));
+            if (!failed) {
+                used = k;
+                break;
+            }
+        }
+        PSIPM_CUDA(cudaEventRecord(h->ev1, st));
+        PSIPM_CUDA(cudaEventSynchronize(h->ev1));
+        float ms = 0.f;
+        PSIPM_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        h->factor_seconds = ms * 1e-3;
+        if (shift_index) *shift_index = used;
+        if (info) {
+            info->nsupernodes = s.ns;
+            info->nlevels = s.nlevels;
+            info->max_front = s.max_front;
+            info->symbolic_analyses = h->n_symbolic;
+            info->nnz_factor = s.nnz_L;
+            info->flops = s.flops;
+            info->symbolic_seconds = h->symbolic_seconds;
+            info->factor_seconds = h->factor_seconds;
+        }
+        if (used < 0) {
+            h->have_factor = false;
+            throw Failure(PSIPM_ERR_NOT_PD, "Cholesky failed even with a 1e-2 shift");
+        }
+        for (int sn : h->solve_big_sn) {
+            const int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
+            const int c = s.sn_first[sn + 1] - s.sn_first[sn];
+            dim3 grid((c + 31) / 32, (r + 31) / 32), block(32, 8);
+            LAUNCH(h, k_transpose_panel<double><<<grid, block, 0, st>>>(h->f64.G.p + s.panel_off[sn], r, c,
+                                                                       h->f64.GT.p + h->gt_off_host[sn]));
+        }
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        h->have_factor = true;
+    });
+    return status;
+}
+
+int psipm_apply(psipm_handle* h, const double* r, double* z) {
+    if (!r || !z) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_factor, PSIPM_ERR_STATE, "apply before a successful factor");
+        PcgArgs<double> a = pcg_args(h);
+        h->r1.upload(r, h->m, h->stream);
+        h->r2.reserve(h->m);
+        const double* in = h->r1.p;
+        double* outp = h->r2.p;
+        void* args[] = {&a, (void*)&in, (void*)&outp};
+        launch_coop(h, (const void*)k_apply<double>, args);
+        copy_out(h, z, h->r2.p, h->m);
+    });
+}
+
+int psipm_matvec(psipm_handle* h, const double* v, double* y) {
+    if (!v || !y) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_theta, PSIPM_ERR_STATE, "matvec before set_theta");
+        PcgArgs<double> a = pcg_args(h);
+        PSIPM_CUDA(cudaMemcpyAsync(h->p64.p.p, v, h->m * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        void* args[] = {&a};
+        launch_coop(h, (const void*)k_matvec<double>, args);
+        copy_out(h, y, h->p64.q.p, h->m);
+    });
+}
+
+int psipm_pcg(psipm_handle* h, const double* rhs, double tol, int32_t maxit, int32_t variant, int32_t replacement,
+              double gap_tolerance, double* x, double* residual, double* alphas, double* betas, double* history,
+              psipm_pcg_info* info) {
+    if (!rhs || !x || maxit < 0 || (variant != PSIPM_PCG_SPECTRAL && variant != PSIPM_PCG_HSD))
+        return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        h->p64.rhs.upload(rhs, h->m, h->stream);
+        psipm_pcg_info local;
+        run_pcg(h, h->p64.rhs.p, tol, maxit, variant, replacement, gap_tolerance, &local);
+        copy_out(h, x, h->p64.x.p, h->m);
+        copy_out(h, residual, h->p64.tr.p, h->m);
+        copy_out(h, alphas, h->alphas.p, local.n_alpha);
+        copy_out(h, betas, h->betas.p, local.n_beta);
+        copy_out(h, history, h->history.p, local.n_history);
+        if (info) *info = local;
+    });
+}
+
+}  // extern "C"
+
+// ---- H1 solve --------------------------------------------------------------
+namespace {
+
+__global__ void k_div(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                      double* __restrict__ out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[i] / b[i];
+}
+
+// out_i = b_i - sum_j A_ij v_j   (A in CSR)
+__global__ void k_rhs(int m, const int* __restrict__ ptr, const int* __restrict__ idx,
+                      const double* __restrict__ val, const double* __restrict__ v,
+                      const double* __restrict__ b, double* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    double s = 0.0;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) s += val[k] * v[idx[k]];
+    out[i] = b[i] - s;
+}
+
+// dx_j = wr1_j + (sum_i A_ij dy_i) / theta_j
+__global__ void k_dx(long long n, const int* __restrict__ ptr, const int* __restrict__ idx,
+                     const double* __restrict__ val, const double* __restrict__ dy,
+                     const double* __restrict__ wr1, const double* __restrict__ theta,
+                     double* __restrict__ dx) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double s = 0.0;
+    for (int k = ptr[j]; k < ptr[j + 1]; ++k) s += val[k] * dy[idx[k]];
+    dx[j] = wr1[j] + s / theta[j];
+}
+
+void solve_device(psipm_handle* h, const double* r1d, const double* r2d, double tol, int maxit, int variant,
+                  int replacement, double gap_tol, double* dxd, psipm_pcg_info* info) {
+    const int64_t m = h->m, n = h->n;
+    cudaStream_t st = h->stream;
+    h->wr1.reserve(n);
+    h->p64.rhs.reserve(m);
+    LAUNCH(h, k_div<<<blocks_for(n, 256), 256, 0, st>>>(n, r1d, h->theta.p, h->wr1.p));
+    LAUNCH(h, k_rhs<<<blocks_for(m, 256), 256, 0, st>>>((int)m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->wr1.p,
+                                                         r2d, h->p64.rhs.p));
+    run_pcg(h, h->p64.rhs.p, tol, maxit, variant, replacement, gap_tol, info);
+    LAUNCH(h, k_dx<<<blocks_for(n, 256), 256, 0, st>>>(n, h->at_ptr.p, h->at_idx.p, h->at_val.p, h->p64.x.p,
+                                                        h->wr1.p, h->theta.p, dxd));
+}
+
+}  // namespace
+
+extern "C" {
+
+int psipm_solve(psipm_handle* h, const double* r1, const double* r2, double tol, int32_t maxit, int32_t variant,
+                int32_t replacement, double gap_tolerance, double* dx, double* dy, double* residual, double* alphas,
+                double* betas, double* history, psipm_pcg_info* info) {
+    if (!r1 || !r2 || !dx || !dy || maxit < 0) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_factor, PSIPM_ERR_STATE, "solve before a successful factor");
+        h->r1.upload(r1, h->n, h->stream);
+        h->r2.upload(r2, h->m, h->stream);
+        h->dx.reserve(h->n);
+        psipm_pcg_info local;
+        solve_device(h, h->r1.p, h->r2.p, tol, maxit, variant, replacement, gap_tolerance, h->dx.p, &local);
+        copy_out(h, dx, h->dx.p, h->n);
+        copy_out(h, dy, h->p64.x.p, h->m);
+        copy_out(h, residual, h->p64.tr.p, h->m);
+        copy_out(h, alphas, h->alphas.p, local.n_alpha);
+        copy_out(h, betas, h->betas.p, local.n_beta);
+        copy_out(h, history, h->history.p, local.n_history);
+        if (info) *info = local;
+    });
+}
+
+int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev, double tol, int32_t maxit,
+                    int32_t variant, int32_t replacement, double gap_tolerance, double* dx_dev, double* dy_dev,
+                    psipm_pcg_info* info) {
+    if (!r1_dev || !r2_dev || !dx_dev || !dy_dev || maxit < 0) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_factor, PSIPM_ERR_STATE, "solve before a successful factor");
+        solve_device(h, r1_dev, r2_dev, tol, maxit, variant, replacement, gap_tolerance, dx_dev, info);
+        PSIPM_CUDA(cudaMemcpyAsync(dy_dev, h->p64.x.p, h->m * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    });
+}
+
+int64_t psipm_kernel_launches(const psipm_handle* h) { return h ? h->launches : -1; }
+
+int psipm_timer_start(psipm_handle* h) {
+    return guarded(h, [&]() { PSIPM_CUDA(cudaEventRecord(h->tv0, h->stream)); });
+}
+
+int psipm_timer_stop(psipm_handle* h, double* seconds) {
+    if (!seconds) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        PSIPM_CUDA(cudaEventRecord(h->tv1, h->stream));
+        PSIPM_CUDA(cudaEventSynchronize(h->tv1));
+        float ms = 0.f;
+        PSIPM_CUDA(cudaEventElapsedTime(&ms, h->tv0, h->tv1));
+        *seconds = ms * 1e-3;
+    });
+}
+
+int psipm_set_profiling(psipm_handle* h, int32_t on) {
+    (void)on;
+    return h ? PSIPM_OK : PSIPM_ERR_ARGUMENT;
+}
+
+}  // extern "C"

@@ -249,6 +249,188 @@ void nested_dissection(const Graph& g, int32_t leaf, std::vector<int32_t>& order
     }
 }
 
+
+// Approximate minimum degree on the quotient graph (Amestoy, Davis & Duff,
+// SIAM J. Matrix Anal. Appl. 17(4), 1996): elements absorb the elements of
+// the pivot, external degrees are bounded by the AMD approximation, and
+// indistinguishable variables are merged into supervariables by hashing.
+void amd_order(const Graph& g, std::vector<int32_t>& order) {
+    const int32_t n = g.n;
+    order.clear();
+    order.reserve(n);
+    enum : int8_t { VAR = 0, ELEM = 1, ABSORBED = 2, MERGED = 3 };
+    std::vector<std::vector<int32_t>> V(n), E(n), L(n), merged(n);
+    std::vector<int32_t> nv(n, 1);
+    std::vector<int64_t> deg(n, 0);
+    std::vector<int8_t> status(n, VAR);
+    std::vector<int64_t> wval(n, 0);
+    std::vector<int32_t> wstamp(n, -1), mark(n, -1);
+    for (int32_t i = 0; i < n; ++i) {
+        V[i].assign(g.adj.begin() + g.xadj[i], g.adj.begin() + g.xadj[i + 1]);
+        deg[i] = (int64_t)V[i].size();
+    }
+    // degree buckets (doubly linked)
+    std::vector<int32_t> head(n + 1, -1), nxt(n, -1), prv(n, -1);
+    auto bucket_of = [&](int32_t i) { return (int32_t)std::min<int64_t>(deg[i], n); };
+    auto insert = [&](int32_t i) {
+        int32_t d = bucket_of(i);
+        nxt[i] = head[d];
+        prv[i] = -1;
+        if (head[d] >= 0) prv[head[d]] = i;
+        head[d] = i;
+    };
+    auto remove = [&](int32_t i) {
+        int32_t d = bucket_of(i);
+        if (prv[i] >= 0)
+            nxt[prv[i]] = nxt[i];
+        else
+            head[d] = nxt[i];
+        if (nxt[i] >= 0) prv[nxt[i]] = prv[i];
+        nxt[i] = prv[i] = -1;
+    };
+    for (int32_t i = 0; i < n; ++i) insert(i);
+    int64_t eliminated = 0;
+    int32_t mindeg = 0, tag = 0, step = 0;
+    std::vector<int32_t> Lp;
+    std::vector<std::pair<uint64_t, int32_t>> hashes;
+    while (eliminated < n) {
+        while (mindeg <= n && head[mindeg] < 0) ++mindeg;
+        if (mindeg > n) break;
+        const int32_t p = head[mindeg];
+        remove(p);
+        ++tag;
+        ++step;
+        mark[p] = tag;
+        Lp.clear();
+        for (int32_t e : E[p]) {
+            if (status[e] != ELEM) continue;
+            for (int32_t v : L[e])
+                if (status[v] == VAR && mark[v] != tag) {
+                    mark[v] = tag;
+                    Lp.push_back(v);
+                }
+            status[e] = ABSORBED;
+            std::vector<int32_t>().swap(L[e]);
+        }
+        for (int32_t v : V[p])
+            if (status[v] == VAR && mark[v] != tag) {
+                mark[v] = tag;
+                Lp.push_back(v);
+            }
+        status[p] = ELEM;
+        std::vector<int32_t>().swap(V[p]);
+        std::vector<int32_t>().swap(E[p]);
+        eliminated += nv[p];
+        order.push_back(p);
+        for (int32_t q : merged[p]) order.push_back(q);
+        std::vector<int32_t>().swap(merged[p]);
+        int64_t degLp = 0;
+        for (int32_t i : Lp) degLp += nv[i];
+        // prune the adjacency of every variable of the new element
+        for (int32_t i : Lp) {
+            remove(i);
+            std::vector<int32_t>& Ei = E[i];
+            size_t w = 0;
+            for (int32_t e : Ei)
+                if (status[e] == ELEM) Ei[w++] = e;
+            Ei.resize(w);
+            Ei.push_back(p);
+            std::vector<int32_t>& Vi = V[i];
+            w = 0;
+            for (int32_t v : Vi)
+                if (status[v] == VAR && mark[v] != tag) Vi[w++] = v;
+            Vi.resize(w);
+        }
+        // |Le \ Lp| for the other elements touching Lp
+        for (int32_t i : Lp)
+            for (int32_t e : E[i]) {
+                if (e == p) continue;
+                if (wstamp[e] != step) {
+                    wstamp[e] = step;
+                    std::vector<int32_t>& Le = L[e];
+                    size_t w = 0;
+                    int64_t size = 0;
+                    for (int32_t v : Le)
+                        if (status[v] == VAR) {
+                            Le[w++] = v;
+                            size += nv[v];
+                        }
+                    Le.resize(w);
+                    wval[e] = size;
+                }
+                wval[e] -= nv[i];
+            }
+        // approximate external degrees, aggressive absorption
+        for (int32_t i : Lp) {
+            int64_t dext = degLp - nv[i];
+            for (int32_t v : V[i]) dext += nv[v];
+            for (int32_t e : E[i]) {
+                if (e == p) continue;
+                if (wval[e] <= 0 && status[e] == ELEM) {
+                    status[e] = ABSORBED;  // e is a subset of Lp
+                    std::vector<int32_t>().swap(L[e]);
+                    continue;
+                }
+                if (status[e] == ELEM) dext += wval[e];
+            }
+            int64_t bound = deg[i] + degLp - nv[i];
+            deg[i] = std::max<int64_t>(0, std::min<int64_t>({dext, bound, (int64_t)n - eliminated}));
+        }
+        // supervariables: identical (V, E) among Lp
+        hashes.clear();
+        for (int32_t i : Lp) {
+            std::vector<int32_t>& Ei = E[i];
+            size_t w = 0;
+            for (int32_t e : Ei)
+                if (status[e] == ELEM) Ei[w++] = e;
+            Ei.resize(w);
+            std::sort(Ei.begin(), Ei.end());
+            std::sort(V[i].begin(), V[i].end());
+            uint64_t h = 1469598103934665603ull;
+            for (int32_t v : V[i]) h = (h ^ (uint64_t)v) * 1099511628211ull;
+            h ^= 0x9e3779b97f4a7c15ull;
+            for (int32_t e : Ei) h = (h ^ (uint64_t)e) * 1099511628211ull;
+            hashes.emplace_back(h, i);
+        }
+        std::sort(hashes.begin(), hashes.end());
+        for (size_t a = 0; a < hashes.size();) {
+            size_t b = a;
+            while (b < hashes.size() && hashes[b].first == hashes[a].first) ++b;
+            for (size_t x = a; x < b; ++x) {
+                int32_t i = hashes[x].second;
+                if (status[i] != VAR) continue;
+                for (size_t y = x + 1; y < b; ++y) {
+                    int32_t j = hashes[y].second;
+                    if (status[j] != VAR) continue;
+                    if (V[i] == V[j] && E[i] == E[j]) {
+                        nv[i] += nv[j];
+                        merged[i].push_back(j);
+                        for (int32_t q : merged[j]) merged[i].push_back(q);
+                        std::vector<int32_t>().swap(merged[j]);
+                        deg[i] = std::max<int64_t>(0, deg[i] - nv[j]);
+                        nv[j] = 0;
+                        status[j] = MERGED;
+                        std::vector<int32_t>().swap(V[j]);
+                        std::vector<int32_t>().swap(E[j]);
+                    }
+                }
+            }
+            a = b;
+        }
+        {
+            size_t w = 0;
+            for (int32_t i : Lp)
+                if (status[i] == VAR) Lp[w++] = i;
+            Lp.resize(w);
+        }
+        L[p] = Lp;
+        for (int32_t i : Lp) {
+            insert(i);
+            mindeg = std::min(mindeg, bucket_of(i));
+        }
+    }
+}
+
 }  // namespace
 
 int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* rowidx,
@@ -268,8 +450,19 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
     if (opt.ordering == 1) {
         order.resize(m);
         std::iota(order.begin(), order.end(), 0);
-    } else {
+    } else if (opt.ordering == 2) {
         nested_dissection(g, std::max(2, opt.leaf_size), order);
+    } else {
+        amd_order(g, order);
+    }
+    {
+        // the ordering must be a permutation
+        std::vector<char> seen(m, 0);
+        if ((int32_t)order.size() != m) return -4;
+        for (int32_t v : order) {
+            if (v < 0 || v >= m || seen[v]) return -5;
+            seen[v] = 1;
+        }
     }
     std::vector<int32_t> iperm(m);
     for (int32_t k = 0; k < m; ++k) iperm[order[k]] = k;

@@ -7,7 +7,8 @@
 // whenever the pattern of P changes.  Here the same event (a new core) runs
 // this analysis:
 //   1. pattern of P from the core columns of A,
-//   2. nested-dissection ordering (BFS level-structure separators),
+//   2. fill-reducing ordering: approximate minimum degree (default) or
+//      nested dissection by BFS level-structure separators,
 //   3. elimination tree, postorder, column counts (row-subtree method),
 //   4. fundamental supernodes + relaxed amalgamation,
 //   5. supernode row structures, extend-add maps, a height-level schedule,
@@ -80,7 +81,7 @@ struct SymbolicOptions {
     int32_t relax_small = 4;       // always merge supernodes up to this many columns
     int32_t relax_medium = 16;     // merge up to this many columns if zeros <= 80%
     int32_t relax_large = 48;      // merge up to this many columns if zeros <= 10%
-    int32_t ordering = 0;          // 0 nested dissection, 1 natural (tests)
+    int32_t ordering = 0;          // 0 approximate minimum degree, 1 natural, 2 nested dissection
 };
 
 // Build the symbolic factor for the core columns `core` (sorted, global

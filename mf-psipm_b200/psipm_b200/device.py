@@ -1,0 +1,203 @@
+"""One LP's device state: a thin Python owner of a ``psipm_handle``.
+
+Every method is one C-ABI call (include/psipm_b200.h); arrays cross the
+boundary as contiguous NumPy buffers.  A nonzero status raises
+:class:`DeviceError`, whose ``status`` is the library's code; the KKT
+wrappers translate it into the reference's ``KKTSolveError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Tuple
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from ._lib import f64, i64, ptr
+
+
+class DeviceError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_lib.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+@dataclass
+class PcgResult:
+    x: np.ndarray
+    info: int
+    iterations: int
+    matvecs: int
+    replacements: int
+    residual_checks: int
+    relative_residual: float
+    ok: bool
+    alphas: np.ndarray
+    betas: np.ndarray
+    history: np.ndarray
+    residual: Optional[np.ndarray]
+    seconds: float
+    refinements: int = 0
+    phase_seconds: tuple = (0.0, 0.0, 0.0, 0.0)
+
+
+class NormalEquationsDevice:
+    """Device-resident ``A``, weights, active core, factor and PCG workspace."""
+
+    def __init__(self, A: sp.csc_matrix, device: int = 0, precision: int = _lib.FP64):
+        self.lib = _lib.load()
+        A = sp.csc_matrix(A)
+        A.sum_duplicates()
+        A.sort_indices()
+        self.A = A
+        self.m, self.n = A.shape
+        self._colptr = i64(A.indptr)
+        self._rowidx = np.ascontiguousarray(A.indices, dtype=np.int32)
+        self._values = f64(A.data)
+        handle = ctypes.c_void_p()
+        status = self.lib.psipm_create(self.m, self.n, A.nnz, ptr(self._colptr), ptr(self._rowidx),
+                                       ptr(self._values), int(device), int(precision),
+                                       ctypes.byref(handle))
+        if status != _lib.OK:
+            message = self.lib.psipm_last_error(handle).decode() if handle.value else ""
+            if handle.value:
+                self.lib.psipm_destroy(handle)
+            if status == _lib.ERR_CUDA:
+                raise _lib.GpuUnavailable(f"CUDA initialisation failed: {message}")
+            raise DeviceError(status, message)
+        self.h = handle
+        ncand = self.lib.psipm_num_candidates(self.h)
+        self.candidates = np.empty(ncand, dtype=np.int64)
+        self._check(self.lib.psipm_get_candidates(self.h, ptr(self.candidates)))
+        self.precision = precision
+
+    # -- plumbing -------------------------------------------------------------
+    def _check(self, status: int) -> None:
+        if status != _lib.OK:
+            raise DeviceError(status, self.lib.psipm_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.psipm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.psipm_kernel_launches(self.h))
+
+    def timer_start(self) -> None:
+        self._check(self.lib.psipm_timer_start(self.h))
+
+    def timer_stop(self) -> float:
+        out = ctypes.c_double()
+        self._check(self.lib.psipm_timer_stop(self.h, ctypes.byref(out)))
+        return float(out.value)
+
+    # -- operations -----------------------------------------------------------
+    def set_theta(self, theta: np.ndarray, delta: float) -> None:
+        theta = f64(theta)
+        if theta.shape != (self.n,):
+            raise ValueError("theta has the wrong dimension")
+        self._check(self.lib.psipm_set_theta(self.h, ptr(theta), float(delta)))
+
+    def scores(self, fill_weight: float, want: bool = True, want_diag: bool = False):
+        out = np.empty(self.candidates.size) if want else None
+        diag = np.empty(self.m) if want_diag else None
+        self._check(self.lib.psipm_scores(self.h, float(fill_weight), ptr(out), ptr(diag)))
+        return out, diag
+
+    def refresh_core(self, target: int, retention: float, stable: bool,
+                     mandatory_local: np.ndarray) -> Tuple[np.ndarray, float]:
+        mandatory_local = i64(mandatory_local)
+        core = np.empty(max(1, self.candidates.size), dtype=np.int64)
+        ncore = ctypes.c_int64()
+        retained = ctypes.c_double()
+        self._check(self.lib.psipm_refresh_core(
+            self.h, int(target), float(retention), int(bool(stable)), ptr(mandatory_local),
+            mandatory_local.size, ptr(core), ctypes.byref(ncore), ctypes.byref(retained)))
+        return core[: ncore.value].copy(), float(retained.value)
+
+    def set_core(self, core: np.ndarray) -> None:
+        core = i64(core)
+        self._check(self.lib.psipm_set_core(self.h, ptr(core), core.size))
+
+    def top_k(self, scores: np.ndarray, count: int, mask: Optional[np.ndarray] = None) -> np.ndarray:
+        scores = f64(scores)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+        out = np.empty(max(1, int(count)), dtype=np.int64)
+        nout = ctypes.c_int64()
+        self._check(self.lib.psipm_top_k(self.h, ptr(scores), scores.size, ptr(m), int(count),
+                                         ptr(out), ctypes.byref(nout)))
+        return out[: nout.value].copy()
+
+    def factor(self, delta: float, start_shift: int = 0):
+        shift = ctypes.c_int32(-1)
+        info = _lib.FactorInfo()
+        status = self.lib.psipm_factor(self.h, float(delta), int(start_shift), ctypes.byref(shift),
+                                       ctypes.byref(info))
+        if status != _lib.OK:
+            raise DeviceError(status, self.lib.psipm_last_error(self.h).decode())
+        return int(shift.value), info
+
+    def apply(self, r: np.ndarray) -> np.ndarray:
+        r = f64(r)
+        z = np.empty(self.m)
+        self._check(self.lib.psipm_apply(self.h, ptr(r), ptr(z)))
+        return z
+
+    def matvec(self, v: np.ndarray) -> np.ndarray:
+        v = f64(v)
+        y = np.empty(self.m)
+        self._check(self.lib.psipm_matvec(self.h, ptr(v), ptr(y)))
+        return y
+
+    def pcg(self, rhs, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100, gap_tolerance=0.1,
+            want_residual=False) -> PcgResult:
+        rhs = f64(rhs)
+        x = np.empty(self.m)
+        res = np.empty(self.m) if want_residual else None
+        alphas = np.empty(max(1, maxit))
+        betas = np.empty(max(1, maxit))
+        history = np.empty(maxit + 2)
+        info = _lib.PcgInfo()
+        self._check(self.lib.psipm_pcg(self.h, ptr(rhs), float(tol), int(maxit), int(variant),
+                                       int(replacement), float(gap_tolerance), ptr(x), ptr(res),
+                                       ptr(alphas), ptr(betas), ptr(history), ctypes.byref(info)))
+        return self._result(x, info, alphas, betas, history, res)
+
+    def solve(self, r1, r2, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100, gap_tolerance=0.1,
+              want_residual=False):
+        r1 = f64(r1)
+        r2 = f64(r2)
+        dx = np.empty(self.n)
+        dy = np.empty(self.m)
+        res = np.empty(self.m) if want_residual else None
+        alphas = np.empty(max(1, maxit))
+        betas = np.empty(max(1, maxit))
+        history = np.empty(maxit + 2)
+        info = _lib.PcgInfo()
+        self._check(self.lib.psipm_solve(self.h, ptr(r1), ptr(r2), float(tol), int(maxit), int(variant),
+                                         int(replacement), float(gap_tolerance), ptr(dx), ptr(dy),
+                                         ptr(res), ptr(alphas), ptr(betas), ptr(history),
+                                         ctypes.byref(info)))
+        return dx, self._result(dy, info, alphas, betas, history, res)
+
+    @staticmethod
+    def _result(x, info, alphas, betas, history, res) -> PcgResult:
+        return PcgResult(
+            x=x, info=int(info.info), iterations=int(info.iterations), matvecs=int(info.matvecs),
+            replacements=int(info.replacements), residual_checks=int(info.residual_checks),
+            relative_residual=float(info.relative_residual), ok=bool(info.ok),
+            alphas=alphas[: info.n_alpha].copy(), betas=betas[: info.n_beta].copy(),
+            history=history[: info.n_history].copy(), residual=res, seconds=float(info.seconds),
+            refinements=int(info.refinements), phase_seconds=tuple(float(v) for v in info.phase_seconds),
+        )
