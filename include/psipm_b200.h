@@ -171,6 +171,11 @@ int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev,
  * an event; stop records a second one, waits for it and returns the elapsed
  * seconds.  Everything the handle launches in between is inside the interval. */
 int psipm_timer_start(psipm_handle* h);
+/* One preconditioner apply with a %globaltimer stamp after every grid barrier
+ * (stamps[0] at entry; *count stamps written, at most cap), and the average
+ * cost of one grid barrier of the persistent kernels in *barrier_ns (may be NULL). */
+int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t* stamps, int32_t cap,
+                            int32_t* count, int32_t* barrier_ns);
 int psipm_timer_stop(psipm_handle* h, double* seconds);
 /* Kernels launched by this handle since creation (all of them are this
  * library's own kernels). */

@@ -38,7 +38,7 @@ void read_thresholds() {
     if (const char* v = std::getenv("PSIPM_BIG_FRONT")) kBigFront = std::max(1, std::atoi(v));
     if (const char* v = std::getenv("PSIPM_BIG_SOLVE")) kBigSolve = std::max(1, std::atoi(v));
 }
-constexpr int kRowsPerTask = 8;
+
 
 template <typename T>
 struct FactorStore {
@@ -295,7 +295,7 @@ PcgArgs<double> pcg_args(psipm_handle* h) {
         pc.fvec = h->f64.fvec.p;
         pc.bvec = h->f64.bvec.p;
         pc.GT = h->f64.GT.p;
-        pc.gt_off = h->gt_off_d.p;
+        pc.gt_off = h->s_panel_off.p;
     }
     PcgStore<double>& st = h->p64;
     const int64_t m = h->m, n = h->n;
@@ -399,38 +399,38 @@ void analyse(psipm_handle* h) {
     h->front_total = fmax_total;
     h->front_off_host = foff;
     up64(h->s_front_off, foff);
-    // triangular-solve tasks per level.  Small supernodes: one warp per 32
-    // rows (forward) / 32 columns (backward), front vector staged in shared
-    // memory.  Big supernodes (c >= kBigSolve): a pre-phase assembles the
-    // vectors in global memory, then warps take kRowsPerTask rows each.
+    // triangular-solve tasks per level (kernels_pcg.cuh, prec_apply):
+    // pre-phase chunks of 64 front positions, then 2-D GEMV tasks of
+    // kApplyRows rows x kApplyChunk contraction entries, all-zero blocks of
+    // the triangular L11^{-1} skipped.
     std::vector<int4> ft, bt, fp, bp;
     h->fwd_ptr.assign(s.nlevels + 1, 0);
     h->bwd_ptr.assign(s.nlevels + 1, 0);
     h->fpre_ptr.assign(s.nlevels + 1, 0);
     h->bpre_ptr.assign(s.nlevels + 1, 0);
-    h->solve_big_sn.clear();
-    h->gt_off_host.assign(s.ns + 1, 0);
-    int64_t gt_total = 0;
     for (int l = 0; l < s.nlevels; ++l) {
         for (int q = s.level_ptr[l]; q < s.level_ptr[l + 1]; ++q) {
             int sn = s.level_sn[q];
             int c = s.sn_first[sn + 1] - s.sn_first[sn];
             int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
-            if (c >= kBigSolve) {
-                h->solve_big_sn.push_back(sn);
-                h->gt_off_host[sn] = gt_total;
-                gt_total += (int64_t)r * c;
-                for (int p0 = 0; p0 < r; p0 += 32) {
-                    fp.push_back(make_int4(sn, p0, std::min(r, p0 + 32), 0));
-                    bp.push_back(make_int4(sn, p0, std::min(r, p0 + 32), 0));
+            for (int p0 = 0; p0 < r; p0 += 64) {
+                fp.push_back(make_int4(sn, p0, std::min(r, p0 + 64), 0));
+                bp.push_back(make_int4(sn, p0, std::min(r, p0 + 64), 0));
+            }
+            for (int i0 = 0; i0 < r; i0 += kApplyRows) {
+                const int i1 = std::min(r, i0 + kApplyRows);
+                for (int j0 = 0; j0 < c; j0 += kApplyChunk) {
+                    if (i1 - 1 < c && j0 > i1 - 1) break;  // above the diagonal of L11^{-1}
+                    ft.push_back(make_int4(sn, i0, i1, j0));
                 }
-                for (int r0 = 0; r0 < r; r0 += kRowsPerTask)
-                    ft.push_back(make_int4(sn, r0, std::min(r, r0 + kRowsPerTask), 2));
-                for (int j0 = 0; j0 < c; j0 += kRowsPerTask)
-                    bt.push_back(make_int4(sn, j0, std::min(c, j0 + kRowsPerTask), 2));
-            } else {
-                for (int r0 = 0; r0 < r; r0 += 32) ft.push_back(make_int4(sn, r0, std::min(r, r0 + 32), 0));
-                for (int j0 = 0; j0 < c; j0 += 32) bt.push_back(make_int4(sn, j0, std::min(c, j0 + 32), 0));
+            }
+            for (int j0 = 0; j0 < c; j0 += kApplyRows) {
+                const int j1 = std::min(c, j0 + kApplyRows);
+                for (int i0 = 0; i0 < r; i0 += kApplyChunk) {
+                    const int i1 = std::min(r, i0 + kApplyChunk);
+                    if (i1 - 1 < j0) continue;  // rows above the block's first column
+                    bt.push_back(make_int4(sn, j0, j1, i0));
+                }
             }
         }
         h->fwd_ptr[l + 1] = (int)ft.size();
@@ -442,11 +442,7 @@ void analyse(psipm_handle* h) {
     h->bpre_ptr_d.upload(h->bpre_ptr, st);
     h->fpre_tasks_d.upload(fp, st);
     h->bpre_tasks_d.upload(bp, st);
-    {
-        std::vector<long long> go(h->gt_off_host.begin(), h->gt_off_host.end());
-        h->gt_off_d.upload(go, st);
-    }
-    h->f64.GT.reserve(std::max<int64_t>(1, gt_total));
+    h->f64.GT.reserve(std::max<int64_t>(1, s.panel_total));
     h->f64.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
     h->f64.bvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
     h->small_ptr.assign(s.nlevels + 1, 0);
@@ -539,6 +535,8 @@ void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
                       F, r, c, fa.update + s.update_off[sn]));
     }
     LAUNCH(h, k_g_trsm<T><<<blocks_for(r, 32), 256, 0, st>>>(F, r, c, fa.G + s.panel_off[sn]));
+    dim3 tgrid((c + 31) / 32, (r + 31) / 32), tblock(32, 8);
+    LAUNCH(h, k_transpose_panel<T><<<tgrid, tblock, 0, st>>>(fa.G + s.panel_off[sn], r, c, fa.GT + s.panel_off[sn]));
 }
 
 // ---------------------------------------------------------------------------
@@ -743,7 +741,10 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
         PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_matvec<double>, kPcgThreads, 0));
         per_sm = std::min(std::min(per_sm, per_sm2), per_sm3);
         require(per_sm >= 1, PSIPM_ERR_UNSUPPORTED, "PCG kernel does not fit on an SM");
-        h->coop_blocks = std::min(per_sm, 2) * h->num_sms;
+        // blocks per SM of the persistent kernels (PSIPM_BLOCKS_PER_SM overrides)
+        int want = 4;
+        if (const char* v = std::getenv("PSIPM_BLOCKS_PER_SM")) want = std::max(1, std::atoi(v));
+        h->coop_blocks = std::min(per_sm, want) * h->num_sms;
         build_matrix(h.get());
     });
     if (rc != PSIPM_OK) {
@@ -948,6 +949,7 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
         fa.ent_rowpos = h->s_ent_rowpos.p;
         fa.ms = h->f64.ms.p;
         fa.G = h->f64.G.p;
+        fa.GT = h->f64.GT.p;
         fa.update = h->f64.update.p;
         fa.front = h->f64.front.p;
         fa.front_off = h->s_front_off.p;
@@ -989,13 +991,6 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
         if (used < 0) {
             h->have_factor = false;
             throw Failure(PSIPM_ERR_NOT_PD, "Cholesky failed even with a 1e-2 shift");
-        }
-        for (int sn : h->solve_big_sn) {
-            const int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
-            const int c = s.sn_first[sn + 1] - s.sn_first[sn];
-            dim3 grid((c + 31) / 32, (r + 31) / 32), block(32, 8);
-            LAUNCH(h, k_transpose_panel<double><<<grid, block, 0, st>>>(h->f64.G.p + s.panel_off[sn], r, c,
-                                                                       h->f64.GT.p + h->gt_off_host[sn]));
         }
         PSIPM_CUDA(cudaStreamSynchronize(st));
         h->have_factor = true;
@@ -1133,6 +1128,46 @@ int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev,
 }
 
 int64_t psipm_kernel_launches(const psipm_handle* h) { return h ? h->launches : -1; }
+
+int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t* stamps, int32_t cap,
+                            int32_t* count, int32_t* barrier_ns) {
+    if (!r || !z || !stamps || cap <= 0 || !count) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_factor, PSIPM_ERR_STATE, "apply before a successful factor");
+        PcgArgs<double> a = pcg_args(h);
+        DevBuf<long long> tr;
+        tr.zero(cap, h->stream);
+        a.pc.trace = tr.p;
+        a.pc.trace_cap = cap;
+        h->r1.upload(r, h->m, h->stream);
+        h->r2.reserve(h->m);
+        const double* in = h->r1.p;
+        double* outp = h->r2.p;
+        void* args[] = {&a, (void*)&in, (void*)&outp};
+        launch_coop(h, (const void*)k_apply<double>, args);
+        copy_out(h, z, h->r2.p, h->m);
+        std::vector<long long> host(cap);
+        PSIPM_CUDA(cudaMemcpyAsync(host.data(), tr.p, cap * sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+        PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+        int n = 0;
+        for (; n < cap && host[n] != 0; ++n) stamps[n] = host[n];
+        *count = n;
+        if (barrier_ns) {
+            DevBuf<long long> out;
+            out.zero(1, h->stream);
+            int iters = 1000;
+            long long* op = out.p;
+            void* bargs[] = {&iters, &op};
+            PSIPM_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_probe, dim3(h->coop_blocks),
+                                                   dim3(kPcgThreads), bargs, 0, h->stream));
+            ++h->launches;
+            long long ns = 0;
+            PSIPM_CUDA(cudaMemcpyAsync(&ns, out.p, sizeof(ns), cudaMemcpyDeviceToHost, h->stream));
+            PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+            *barrier_ns = (int32_t)(ns / iters);
+        }
+    });
+}
 
 int psipm_timer_start(psipm_handle* h) {
     return guarded(h, [&]() { PSIPM_CUDA(cudaEventRecord(h->tv0, h->stream)); });

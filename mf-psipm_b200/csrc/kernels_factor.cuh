@@ -37,6 +37,7 @@ struct FactorArgs {
     double eta = 0.0;       // diagonal shift
     // outputs / work
     T* G = nullptr;
+    T* GT = nullptr;  // transposed panels (c x r row-major), same offsets as G
     T* update = nullptr;
     T* front = nullptr;                  // level workspace
     const long long* front_off = nullptr;  // per supernode, within the level workspace
@@ -191,6 +192,14 @@ __global__ void __launch_bounds__(kFactorThreads) k_factor_level(FactorArgs<T> a
         T sum = 0;
         for (int k = j; k < c; ++k) sum += F[(long long)k * r + i] * G[(long long)k * c + j];
         G[(long long)i * c + j] = sum;
+    }
+    __syncthreads();
+    // GT = G^T (c x r, row-major)
+    T* GT = a.GT + a.panel_off[s];
+    const long long nrc = (long long)r * c;
+    for (long long q = tid; q < nrc; q += bs) {
+        const int j = (int)(q / r), i = (int)(q % r);
+        GT[q] = G[(long long)i * c + j];
     }
 }
 

@@ -76,6 +76,8 @@ struct PrecLayout {
     T* bvec = nullptr;
     const T* GT = nullptr;             // transposed panels of big supernodes (c x r row-major)
     const long long* gt_off = nullptr;
+    long long* trace = nullptr;  // optional: %globaltimer after every barrier of an apply
+    int trace_cap = 0;
     T* xp = nullptr;
     T* yp = nullptr;
     T* uvec = nullptr;
@@ -241,74 +243,44 @@ __device__ void phase_b2(const PcgArgs<T>& a, int mode, int src, T beta, double 
 }
 
 // ---- preconditioner apply ----------------------------------------------------
+// P^{-1} = Ds Pi^T L^{-T} L^{-1} Pi Ds with L supernodal.  Each supernode s
+// (c pivot columns, r rows) stores G = [L11^{-1} ; L21 L11^{-1}] (r x c,
+// row-major) and its transpose GT (c x r, row-major), so both sweeps are
+// dense matrix-vector products over contiguous rows:
+//   forward  (levels bottom-up):  f = [b_s ; 0] + sum_children u_child
+//                                 x_s = G_top f_top,  u_s = f_bot - G_bot f_top
+//   backward (levels top-down):   v = [x_s ; -y(rows below)]
+//                                 y_s = G^T v
+// Per level and sweep: a pre-phase assembles f (or v) in global memory and
+// initialises the outputs, then 2-D tasks (kApplyRows rows x kApplyChunk
+// contraction entries) accumulate their partial products with atomics.
+constexpr int kApplyRows = 16;
+constexpr int kApplyChunk = 256;
+
+// Four rows against one vector by one warp: lanes stride the contraction
+// index, four independent accumulators, results in every lane.
 template <typename T>
-__device__ void prec_forward_task(const PcgArgs<T>& a, const T* in, int4 task, T* fs) {
-    const PrecLayout<T>& pc = a.pc;
+__device__ __forceinline__ void warp_dot4(const T* __restrict__ m0, const T* __restrict__ m1,
+                                          const T* __restrict__ m2, const T* __restrict__ m3,
+                                          const T* __restrict__ v, int b0, int b1, int b2, int b3,
+                                          int e, T (&out)[4]) {
     const int lane = threadIdx.x & 31;
-    const int s = task.x, r0 = task.y, r1 = task.z;
-    const int first = pc.sn_first[s];
-    const int c = pc.sn_first[s + 1] - first;
-    const long long rb = pc.sn_rowptr[s];
-    const T* __restrict__ Gs = pc.G + pc.panel_off[s];
-    T acc = 0;
-    for (int j0 = 0; j0 < c; j0 += kStageChunk) {
-        const int jn = min(kStageChunk, c - j0);
-        if (r1 <= c && r1 - 1 < j0) break;  // all rows of the task are above this chunk
-        for (int jj = lane; jj < jn; jj += 32) {
-            const int j = j0 + jj, k = first + j;
-            T f = pc.dscp[k] * in[pc.perm[k]];
-            for (long long g = pc.fg_ptr[rb + j]; g < pc.fg_ptr[rb + j + 1]; ++g) f += pc.uvec[pc.fg_idx[g]];
-            fs[jj] = f;
-        }
-        __syncwarp();
-        for (int rr = r0; rr < r1; ++rr) {
-            const int jlim = rr < c ? min(jn, rr - j0 + 1) : jn;
-            T d = 0;
-            const T* __restrict__ grow = Gs + (long long)rr * c + j0;
-            for (int jj = lane; jj < jlim; jj += 32) d += grow[jj] * fs[jj];
-            d = warp_sum(d);
-            if (lane == rr - r0) acc += d;
-        }
-        __syncwarp();
+    T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    const int lo = min(min(b0, b1), min(b2, b3));
+    for (int j = lo + lane; j < e; j += 32) {
+        const T vj = v[j];
+        if (j >= b0) s0 += m0[j] * vj;
+        if (j >= b1) s1 += m1[j] * vj;
+        if (j >= b2) s2 += m2[j] * vj;
+        if (j >= b3) s3 += m3[j] * vj;
     }
-    const int rr = r0 + lane;
-    if (rr < r1) {
-        if (rr < c) {
-            pc.xp[first + rr] = acc;
-        } else {
-            T fb = 0;
-            for (long long g = pc.fg_ptr[rb + rr]; g < pc.fg_ptr[rb + rr + 1]; ++g) fb += pc.uvec[pc.fg_idx[g]];
-            pc.uvec[pc.uvec_off[s] + rr - c] = fb - acc;
-        }
-    }
+    out[0] = warp_sum(s0);
+    out[1] = warp_sum(s1);
+    out[2] = warp_sum(s2);
+    out[3] = warp_sum(s3);
 }
 
-template <typename T>
-__device__ void prec_backward_task(const PcgArgs<T>& a, int4 task) {
-    const PrecLayout<T>& pc = a.pc;
-    const int lane = threadIdx.x & 31;
-    const int s = task.x, j0 = task.y, j1 = task.z;
-    const int first = pc.sn_first[s];
-    const int c = pc.sn_first[s + 1] - first;
-    const long long rb = pc.sn_rowptr[s];
-    const int r = (int)(pc.sn_rowptr[s + 1] - rb);
-    const T* __restrict__ Gs = pc.G + pc.panel_off[s];
-    const int j = j0 + lane;
-    const bool valid = j < j1;
-    T acc = 0;
-    for (int i = j0; i < c; ++i) {
-        const T v = pc.xp[first + i];
-        if (valid) acc += Gs[(long long)i * c + j] * v;
-    }
-    for (int i = c; i < r; ++i) {
-        const T v = pc.yp[pc.sn_rows[rb + i]];
-        if (valid) acc -= Gs[(long long)i * c + j] * v;
-    }
-    if (valid) pc.yp[first + j] = acc;
-}
-
-// Big supernodes (task kind 2): the front vector is assembled in global
-// memory by a pre-phase, then each warp computes a few rows of G f.
+// forward pre-phase: f into fvec, outputs initialised (x_s = 0, u_s = f_bot)
 template <typename T>
 __device__ void prec_forward_pre(const PcgArgs<T>& a, const T* in, int4 task) {
     const PrecLayout<T>& pc = a.pc;
@@ -325,34 +297,60 @@ __device__ void prec_forward_pre(const PcgArgs<T>& a, const T* in, int4 task) {
         }
         for (long long g = pc.fg_ptr[rb + q]; g < pc.fg_ptr[rb + q + 1]; ++g) f += pc.uvec[pc.fg_idx[g]];
         pc.fvec[rb + q] = f;
+        if (q < c)
+            pc.xp[first + q] = 0;
+        else
+            pc.uvec[pc.uvec_off[s] + q - c] = f;
     }
 }
 
+// forward task {s, i0, i1, j0}: rows [i0, i1) of G against f[j0, j0+chunk)
 template <typename T>
-__device__ void prec_forward_rows(const PcgArgs<T>& a, int4 task) {
+__device__ void prec_forward_gemv(const PcgArgs<T>& a, int4 task) {
     const PrecLayout<T>& pc = a.pc;
     const int lane = threadIdx.x & 31;
-    const int s = task.x;
+    const int s = task.x, i0 = task.y, i1 = task.z, j0 = task.w;
     const int first = pc.sn_first[s];
     const int c = pc.sn_first[s + 1] - first;
+    const int j1 = min(c, j0 + kApplyChunk);
     const long long rb = pc.sn_rowptr[s];
     const T* __restrict__ Gs = pc.G + pc.panel_off[s];
     const T* __restrict__ f = pc.fvec + rb;
-    for (int rr = task.y; rr < task.z; ++rr) {
-        const int jlim = rr < c ? rr + 1 : c;
-        const T* __restrict__ grow = Gs + (long long)rr * c;
-        T d = 0;
-        for (int j = lane; j < jlim; j += 32) d += grow[j] * f[j];
-        d = warp_sum(d);
-        if (lane == 0) {
-            if (rr < c)
-                pc.xp[first + rr] = d;
+    for (int i = i0; i < i1; i += 4) {
+        const T* rows[4];
+        int end[4];
+        for (int k = 0; k < 4; ++k) {
+            const int ii = min(i + k, i1 - 1);
+            rows[k] = Gs + (long long)ii * c;
+            end[k] = i + k < i1 ? (ii < c ? min(j1, ii + 1) : j1) : j0;  // G_top is lower triangular
+        }
+        // rows share the loop bound j1; entries past a row's own end are masked
+        T d[4];
+        const int lo = j0;
+        T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int j = lo + lane; j < j1; j += 32) {
+            const T fj = f[j];
+            if (j < end[0]) s0 += rows[0][j] * fj;
+            if (j < end[1]) s1 += rows[1][j] * fj;
+            if (j < end[2]) s2 += rows[2][j] * fj;
+            if (j < end[3]) s3 += rows[3][j] * fj;
+        }
+        d[0] = warp_sum(s0);
+        d[1] = warp_sum(s1);
+        d[2] = warp_sum(s2);
+        d[3] = warp_sum(s3);
+        if (lane < 4 && i + lane < i1) {
+            const int ii = i + lane;
+            const T v = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
+            if (ii < c)
+                atomicAdd(&pc.xp[first + ii], v);
             else
-                pc.uvec[pc.uvec_off[s] + rr - c] = f[rr] - d;
+                atomicAdd(&pc.uvec[pc.uvec_off[s] + ii - c], -v);
         }
     }
 }
 
+// backward pre-phase: v into bvec, y_s = 0
 template <typename T>
 __device__ void prec_backward_pre(const PcgArgs<T>& a, int4 task) {
     const PrecLayout<T>& pc = a.pc;
@@ -361,27 +359,38 @@ __device__ void prec_backward_pre(const PcgArgs<T>& a, int4 task) {
     const int first = pc.sn_first[s];
     const int c = pc.sn_first[s + 1] - first;
     const long long rb = pc.sn_rowptr[s];
-    for (int q = task.y + lane; q < task.z; q += 32)
+    for (int q = task.y + lane; q < task.z; q += 32) {
         pc.bvec[rb + q] = q < c ? pc.xp[first + q] : -pc.yp[pc.sn_rows[rb + q]];
+        if (q < c) pc.yp[first + q] = 0;
+    }
 }
 
+// backward task {s, j0, j1, i0}: columns [j0, j1) of G (rows of GT) against v[i0, i0+chunk)
 template <typename T>
-__device__ void prec_backward_rows(const PcgArgs<T>& a, int4 task) {
+__device__ void prec_backward_gemv(const PcgArgs<T>& a, int4 task) {
     const PrecLayout<T>& pc = a.pc;
     const int lane = threadIdx.x & 31;
-    const int s = task.x;
+    const int s = task.x, j0 = task.y, j1 = task.z, i0 = task.w;
     const int first = pc.sn_first[s];
     const long long rb = pc.sn_rowptr[s];
     const int r = (int)(pc.sn_rowptr[s + 1] - rb);
+    const int i1 = min(r, i0 + kApplyChunk);
     const T* __restrict__ GTs = pc.GT + pc.gt_off[s];
     const T* __restrict__ v = pc.bvec + rb;
-    for (int j = task.y; j < task.z; ++j) {
-        const T* __restrict__ grow = GTs + (long long)j * r;
-        T d = 0;
-        for (int i = (j & ~31) + lane; i < r; i += 32)
-            if (i >= j) d += grow[i] * v[i];
-        d = warp_sum(d);
-        if (lane == 0) pc.yp[first + j] = d;
+    for (int j = j0; j < j1; j += 4) {
+        const T* rows[4];
+        int beg[4];
+        for (int k = 0; k < 4; ++k) {
+            const int jj = min(j + k, j1 - 1);
+            rows[k] = GTs + (long long)jj * r;
+            beg[k] = j + k < j1 ? max(i0, jj) : i1;  // G[i, j] = 0 for i < j
+        }
+        T d[4];
+        warp_dot4(rows[0], rows[1], rows[2], rows[3], v, beg[0], beg[1], beg[2], beg[3], i1, d);
+        if (lane < 4 && j + lane < j1) {
+            const T val = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
+            atomicAdd(&pc.yp[first + j + lane], val);
+        }
     }
 }
 
@@ -390,38 +399,35 @@ __device__ void prec_backward_rows(const PcgArgs<T>& a, int4 task) {
 template <typename T>
 __device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc_rz, T* fs,
                            cgx::grid_group& grid) {
+    (void)fs;
     const PrecLayout<T>& pc = a.pc;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    int ntrace = 0;
+    const bool tracer = pc.trace && blockIdx.x == 0 && threadIdx.x == 0;
+    auto mark = [&]() {
+        if (tracer && ntrace < pc.trace_cap) pc.trace[ntrace++] = global_ns();
+    };
+    mark();
     for (int lev = 0; lev < pc.nlevels; ++lev) {
-        if (pc.fpre_ptr[lev + 1] > pc.fpre_ptr[lev]) {
-            for (int tk = pc.fpre_ptr[lev] + gwarp; tk < pc.fpre_ptr[lev + 1]; tk += nwarps)
-                prec_forward_pre(a, in, pc.fpre_tasks[tk]);
-            grid.sync();
-        }
-        for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps) {
-            const int4 task = pc.fwd_tasks[tk];
-            if (task.w == 2)
-                prec_forward_rows(a, task);
-            else
-                prec_forward_task(a, in, task, fs);
-        }
+        for (int tk = pc.fpre_ptr[lev] + gwarp; tk < pc.fpre_ptr[lev + 1]; tk += nwarps)
+            prec_forward_pre(a, in, pc.fpre_tasks[tk]);
         grid.sync();
+        mark();
+        for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps)
+            prec_forward_gemv(a, pc.fwd_tasks[tk]);
+        grid.sync();
+        mark();
     }
     for (int lev = pc.nlevels - 1; lev >= 0; --lev) {
-        if (pc.bpre_ptr[lev + 1] > pc.bpre_ptr[lev]) {
-            for (int tk = pc.bpre_ptr[lev] + gwarp; tk < pc.bpre_ptr[lev + 1]; tk += nwarps)
-                prec_backward_pre(a, pc.bpre_tasks[tk]);
-            grid.sync();
-        }
-        for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps) {
-            const int4 task = pc.bwd_tasks[tk];
-            if (task.w == 2)
-                prec_backward_rows(a, task);
-            else
-                prec_backward_task(a, task);
-        }
+        for (int tk = pc.bpre_ptr[lev] + gwarp; tk < pc.bpre_ptr[lev + 1]; tk += nwarps)
+            prec_backward_pre(a, pc.bpre_tasks[tk]);
         grid.sync();
+        mark();
+        for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps)
+            prec_backward_gemv(a, pc.bwd_tasks[tk]);
+        grid.sync();
+        mark();
     }
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
@@ -703,6 +709,14 @@ done:
         lap(3);
         for (int k = 0; k < 4; ++k) a.dout[2 + k] = ph[k];
     }
+}
+
+// Grid-barrier cost probe: `count` barriers, nothing else.
+__global__ void k_barrier_probe(int count, long long* out) {
+    cgx::grid_group grid = cgx::this_grid();
+    const long long t0 = global_ns();
+    for (int i = 0; i < count; ++i) grid.sync();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *out = global_ns() - t0;
 }
 
 // Standalone preconditioner apply / operator kernels (cooperative as well)

@@ -106,6 +106,7 @@ SIGNATURES = {
     "psipm_kernel_launches": (_I64, [_P]),
     "psipm_set_profiling": (_I32, [_P, _I32]),
     "psipm_timer_start": (_I32, [_P]),
+    "psipm_debug_apply_trace": (_I32, [_P, _P, _P, _P, _I32, _P, _P]),
     "psipm_timer_stop": (_I32, [_P, _P]),
 }
 
