@@ -184,6 +184,29 @@ int64_t psipm_kernel_launches(const psipm_handle* h);
  * [1] preconditioner apply, [2] vector ops; filled only when profiling is on. */
 int psipm_set_profiling(psipm_handle* h, int32_t on);
 
+/* ---- allocation-free operator product -------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory (a host framework that owns the whole device pool,
+ * code that may not call cudaMalloc/cudaFree because they synchronise the
+ * device, a solver with a fixed, declared memory footprint).
+ *   y = A diag(w) A^T v + delta v
+ * Every argument except `delta` and `stream` is a DEVICE pointer owned by the
+ * caller: A^T in CSR (at_ptr[n+1], at_idx, at_val: i.e. A in CSC) and A in
+ * CSR (a_ptr[m+1], a_idx, a_val), w[n], v[m], y[m].  The intermediate
+ * w o (A^T v) uses a fixed device array inside the library instead of an
+ * allocation, so n may be at most PSIPM_STATIC_SCRATCH_MAX columns
+ * (PSIPM_ERR_ARGUMENT otherwise).  The kernels run on `stream` (a
+ * cudaStream_t, NULL for the default stream) and the call returns without
+ * waiting for them.  The first call on a device looks up the array's device
+ * address and must come before any stream capture.  All calls share the one
+ * array and it keeps the last call's contents (each call writes what it
+ * reads, nothing needs clearing); calls whose kernels overlap on the GPU race. */
+#define PSIPM_STATIC_SCRATCH_MAX (1ll << 20)
+int psipm_normal_matvec_static(int64_t m, int64_t n, const int32_t* at_ptr, const int32_t* at_idx,
+                               const double* at_val, const int32_t* a_ptr, const int32_t* a_idx,
+                               const double* a_val, const double* w, double delta, const double* v,
+                               double* y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

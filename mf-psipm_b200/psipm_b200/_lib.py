@@ -28,6 +28,8 @@ ERR_MEMORY = -7
 ERR_SYMBOLIC = -8
 ERR_UNSUPPORTED = -9
 
+STATIC_SCRATCH_MAX = 1 << 20  # columns, psipm_normal_matvec_static
+
 PCG_SPECTRAL = 0
 PCG_HSD = 1
 FP64 = 0
@@ -106,6 +108,7 @@ SIGNATURES = {
     "psipm_kernel_launches": (_I64, [_P]),
     "psipm_set_profiling": (_I32, [_P, _I32]),
     "psipm_timer_start": (_I32, [_P]),
+    "psipm_normal_matvec_static": (_I32, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P]),
     "psipm_debug_apply_trace": (_I32, [_P, _P, _P, _P, _I32, _P, _P]),
     "psipm_timer_stop": (_I32, [_P, _P]),
 }
