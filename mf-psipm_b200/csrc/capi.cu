@@ -413,6 +413,12 @@ void analyse(psipm_handle* h) {
             int sn = s.level_sn[q];
             int c = s.sn_first[sn + 1] - s.sn_first[sn];
             int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
+            if (r <= kSmallRows && c <= 32) {
+                // whole supernode in one fused warp task (no pre-phase)
+                ft.push_back(make_int4(sn, 0, r, -1));
+                bt.push_back(make_int4(sn, 0, c, -1));
+                continue;
+            }
             for (int p0 = 0; p0 < r; p0 += 64) {
                 fp.push_back(make_int4(sn, p0, std::min(r, p0 + 64), 0));
                 bp.push_back(make_int4(sn, p0, std::min(r, p0 + 64), 0));

@@ -394,13 +394,68 @@ __device__ void prec_backward_gemv(const PcgArgs<T>& a, int4 task) {
     }
 }
 
+// Small supernodes (r <= kSmallRows, c <= 32): one warp does the whole
+// supernode in one task, the vector staged in shared memory and one lane per
+// output, so no pre-phase, no shuffles and no atomics are needed.
+constexpr int kSmallRows = 64;
+
+template <typename T>
+__device__ void prec_forward_small(const PcgArgs<T>& a, const T* in, int s, T* fs) {
+    const PrecLayout<T>& pc = a.pc;
+    const int lane = threadIdx.x & 31;
+    const int first = pc.sn_first[s];
+    const int c = pc.sn_first[s + 1] - first;
+    const long long rb = pc.sn_rowptr[s];
+    const int r = (int)(pc.sn_rowptr[s + 1] - rb);
+    for (int q = lane; q < r; q += 32) {
+        T f = 0;
+        if (q < c) {
+            const int k = first + q;
+            f = pc.dscp[k] * in[pc.perm[k]];
+        }
+        for (long long g = pc.fg_ptr[rb + q]; g < pc.fg_ptr[rb + q + 1]; ++g) f += pc.uvec[pc.fg_idx[g]];
+        fs[q] = f;
+    }
+    __syncwarp();
+    const T* __restrict__ Gs = pc.G + pc.panel_off[s];
+    for (int row = lane; row < r; row += 32) {
+        const int jlim = row < c ? row + 1 : c;
+        const T* __restrict__ g = Gs + (long long)row * c;
+        T d = 0;
+        for (int j = 0; j < jlim; ++j) d += g[j] * fs[j];
+        if (row < c)
+            pc.xp[first + row] = d;
+        else
+            pc.uvec[pc.uvec_off[s] + row - c] = fs[row] - d;
+    }
+    __syncwarp();
+}
+
+template <typename T>
+__device__ void prec_backward_small(const PcgArgs<T>& a, int s, T* fs) {
+    const PrecLayout<T>& pc = a.pc;
+    const int lane = threadIdx.x & 31;
+    const int first = pc.sn_first[s];
+    const int c = pc.sn_first[s + 1] - first;
+    const long long rb = pc.sn_rowptr[s];
+    const int r = (int)(pc.sn_rowptr[s + 1] - rb);
+    for (int q = lane; q < r; q += 32) fs[q] = q < c ? pc.xp[first + q] : -pc.yp[pc.sn_rows[rb + q]];
+    __syncwarp();
+    if (lane < c) {
+        const T* __restrict__ gt = pc.GT + pc.panel_off[s] + (long long)lane * r;
+        T d = 0;
+        for (int i = lane; i < r; ++i) d += gt[i] * fs[i];
+        pc.yp[first + lane] = d;
+    }
+    __syncwarp();
+}
+
 // z = P^{-1} in; acc_rz += in . z.  Ends without a barrier (the caller's
 // reduction provides it).
 template <typename T>
 __device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc_rz, T* fs,
                            cgx::grid_group& grid) {
-    (void)fs;
-    const PrecLayout<T>& pc = a.pc;
+        const PrecLayout<T>& pc = a.pc;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     int ntrace = 0;
@@ -409,23 +464,38 @@ __device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc
         if (tracer && ntrace < pc.trace_cap) pc.trace[ntrace++] = global_ns();
     };
     mark();
+    // task kind (int4.w for fused tasks is -1): fused small supernode or 2-D GEMV
     for (int lev = 0; lev < pc.nlevels; ++lev) {
-        for (int tk = pc.fpre_ptr[lev] + gwarp; tk < pc.fpre_ptr[lev + 1]; tk += nwarps)
-            prec_forward_pre(a, in, pc.fpre_tasks[tk]);
-        grid.sync();
-        mark();
-        for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps)
-            prec_forward_gemv(a, pc.fwd_tasks[tk]);
+        if (pc.fpre_ptr[lev + 1] > pc.fpre_ptr[lev]) {
+            for (int tk = pc.fpre_ptr[lev] + gwarp; tk < pc.fpre_ptr[lev + 1]; tk += nwarps)
+                prec_forward_pre(a, in, pc.fpre_tasks[tk]);
+            grid.sync();
+            mark();
+        }
+        for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps) {
+            const int4 task = pc.fwd_tasks[tk];
+            if (task.w < 0)
+                prec_forward_small(a, in, task.x, fs);
+            else
+                prec_forward_gemv(a, task);
+        }
         grid.sync();
         mark();
     }
     for (int lev = pc.nlevels - 1; lev >= 0; --lev) {
-        for (int tk = pc.bpre_ptr[lev] + gwarp; tk < pc.bpre_ptr[lev + 1]; tk += nwarps)
-            prec_backward_pre(a, pc.bpre_tasks[tk]);
-        grid.sync();
-        mark();
-        for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps)
-            prec_backward_gemv(a, pc.bwd_tasks[tk]);
+        if (pc.bpre_ptr[lev + 1] > pc.bpre_ptr[lev]) {
+            for (int tk = pc.bpre_ptr[lev] + gwarp; tk < pc.bpre_ptr[lev + 1]; tk += nwarps)
+                prec_backward_pre(a, pc.bpre_tasks[tk]);
+            grid.sync();
+            mark();
+        }
+        for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps) {
+            const int4 task = pc.bwd_tasks[tk];
+            if (task.w < 0)
+                prec_backward_small(a, task.x, fs);
+            else
+                prec_backward_gemv(a, task);
+        }
         grid.sync();
         mark();
     }
@@ -454,7 +524,7 @@ __device__ void operator_pass(const PcgArgs<T>& a, const T* v, int src, T beta, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs<T> a) {
+__global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T> a) {
     cgx::grid_group grid = cgx::this_grid();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double scratch[kPcgWarps + 1];
@@ -721,7 +791,7 @@ __global__ void k_barrier_probe(int count, long long* out) {
 
 // Standalone preconditioner apply / operator kernels (cooperative as well)
 template <typename T>
-__global__ void __launch_bounds__(kPcgThreads) k_apply(PcgArgs<T> a, const T* in, T* out) {
+__global__ void __launch_bounds__(kPcgThreads, 3) k_apply(PcgArgs<T> a, const T* in, T* out) {
     cgx::grid_group grid = cgx::this_grid();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* fs = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
@@ -731,7 +801,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_apply(PcgArgs<T> a, const T* in
 
 // y = H v  (mode 0 with src = v copied into p first by the host)
 template <typename T>
-__global__ void __launch_bounds__(kPcgThreads) k_matvec(PcgArgs<T> a) {
+__global__ void __launch_bounds__(kPcgThreads, 3) k_matvec(PcgArgs<T> a) {
     cgx::grid_group grid = cgx::this_grid();
     double acc[3] = {0.0, 0.0, 0.0};
     operator_pass(a, a.p, 0, (T)0, 0, acc, grid);
