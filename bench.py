@@ -217,6 +217,7 @@ def run_ours(args, rank, world, local_rank):
 
     from psipm_b200 import ipm
     from psipm_b200.device import NormalEquationsDevice
+    from psipm_b200.replicas import max_over_ranks
     from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner
 
     torch.cuda.set_device(local_rank)
@@ -259,11 +260,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = dev.kernel_launches - launches0
-    per_step = total / args.steps
-    if dist:
-        t = torch.tensor([per_step], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        per_step = float(t.item())
+    per_step = max_over_ranks(total / args.steps)
     # ---- end to end through the public API, host buffers ----------------------
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -274,10 +271,7 @@ def run_ours(args, rank, world, local_rank):
     h2d = (8 * (n + 1) + 12 * lp.A.nnz) + solver_e2e.h2d_bytes
     d2h = 8 * solver_e2e.candidates.size + solver_e2e.d2h_bytes + 8 * x_host.size * 0
     solver_e2e.close()
-    if dist:
-        t = torch.tensor([e2e], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e = max_over_ranks(e2e)
     peak, peak_kind = measured_peaks()
     achieved = pcg_b / pcg_s / 1e9 if pcg_s > 0 else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

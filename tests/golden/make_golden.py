@@ -37,6 +37,7 @@ INSTANCES = {
     "grid_20x25": ("grid_network", dict(rows=20, cols=25, seed=1000)),
     "cover_m200": ("set_cover", dict(m=200, n=10_000, seed=2000)),
 }
+# plus hsd_m1600 (make_hsd): the V3.1 HSD preconditioner surface
 # the small instances use the stable core path (the exact-preconditioner
 # gate, psipm_stable_preconditioner.py:202-207, would otherwise switch it off)
 OPTIONS = dict(full_preconditioner_row_threshold=10)
@@ -123,6 +124,41 @@ def main():
         np.savez_compressed(path, **out)
         print(f"{name}: {sol.status} obj {sol.obj!r} pcg {sol.pcg_iterations} "
               f"-> {os.path.getsize(path) / 1e6:.2f} MB")
+
+    if args.only in (None, "hsd_m1600"):
+        make_hsd(PS, synthetic)
+
+
+def make_hsd(PS, synthetic):
+    """V3.1 HSD surface: StableColumnPreconditioner.factor + _pcg
+    (psipm_v3_1_hsd.py:823-989, 1015-1063) on a random LP with m > 1500, so
+    the stable core path (not the exact small-row gate) is taken."""
+    import psipm_v3_1_hsd as H
+
+    lp = synthetic.random_lp(1600, 4800, seed=5)
+    A = lp.A
+    rng = np.random.default_rng(20)
+    options = H.V3Options(generic_preconditioner="stable")
+    pre = H.StableColumnPreconditioner(A, options)
+    out = dict(A_data=A.data, A_indices=A.indices, A_indptr=A.indptr, A_shape=np.array(A.shape))
+    for call in range(3):
+        D = np.exp(rng.uniform(-6.0, 6.0, A.shape[1]))
+        delta = 1e-8
+        pre.factor(D, delta)
+        rhs = A @ (D * rng.standard_normal(A.shape[1]))
+
+        def matvec(v, D=D, delta=delta):
+            return A @ (D * (A.T @ v)) + delta * v
+
+        x, it, mv, ok, _ = H._pcg(matvec, rhs, pre, 1e-10, options.pcg_max_iterations, np.inf)
+        pre.record_iterations(it, 0.0, ok)
+        out.update({f"c{call}_D": D, f"c{call}_delta": delta, f"c{call}_rhs": rhs, f"c{call}_x": x,
+                    f"c{call}_iterations": it, f"c{call}_matvecs": mv, f"c{call}_ok": ok,
+                    f"c{call}_core": pre.impl.core.copy(), f"c{call}_n_fact": pre.impl.n_fact})
+    path = os.path.join(HERE, "hsd_m1600.npz")
+    np.savez_compressed(path, **out)
+    print(f"hsd_m1600: iterations {[int(out[f'c{i}_iterations']) for i in range(3)]} "
+          f"-> {os.path.getsize(path) / 1e6:.2f} MB")
 
 
 if __name__ == "__main__":
