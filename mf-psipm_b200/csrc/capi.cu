@@ -115,12 +115,16 @@ struct psipm_handle {
     // numeric
     DevBuf<double> pval, dscp64;
     FactorStore<double> f64;
+    FactorStore<float> f32;          // FP32_REFINED: factor and solve panels in FP32
+    DevBuf<float> at_valf, a_valf, wf;
     bool have_factor = false;
     double factor_seconds = 0.0;
     DevBuf<int> fail;
 
     // PCG
     PcgStore<double> p64;
+    PcgStore<float> p32;
+    DevBuf<double> x64, r64, rhs64, t64, norm64;  // FP64 refinement (FP32_REFINED)
     DevBuf<double> part;
     DevBuf<int> ctrl, iout;
     DevBuf<double> dout, alphas, betas, history;
@@ -200,6 +204,12 @@ void build_matrix(psipm_handle* h) {
     h->a_ptr.upload(a_ptr, h->stream);
     h->a_idx.upload(a_idx, h->stream);
     h->a_val.upload(a_val, h->stream);
+    if (h->precision == PSIPM_FP32_REFINED) {
+        std::vector<float> af(a_val.begin(), a_val.end()), atf(h->val.begin(), h->val.end());
+        h->a_valf.upload(af, h->stream);
+        h->at_valf.upload(atf, h->stream);
+        PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+    }
     // short / long rows
     std::vector<int> shortr, longr, lcp{0}, cb, ce;
     int64_t short_nnz = 0, short_cnt = 0;
@@ -259,20 +269,34 @@ SpmvLayout spmv_layout(psipm_handle* h) {
     return s;
 }
 
-PcgArgs<double> pcg_args(psipm_handle* h) {
-    PcgArgs<double> a;
-    a.sp = spmv_layout<double>(h);
-    a.at_val = h->at_val.p;
-    a.a_val = h->a_val.p;
-    a.w = h->w.p;
-    a.delta = h->delta;
-    PrecLayout<double>& pc = a.pc;
+FactorStore<double>& fstore(psipm_handle* h, const double*) { return h->f64; }
+FactorStore<float>& fstore(psipm_handle* h, const float*) { return h->f32; }
+PcgStore<double>& pstore(psipm_handle* h, const double*) { return h->p64; }
+PcgStore<float>& pstore(psipm_handle* h, const float*) { return h->p32; }
+const double* at_values(psipm_handle* h, const double*) { return h->at_val.p; }
+const float* at_values(psipm_handle* h, const float*) { return h->at_valf.p; }
+const double* a_values(psipm_handle* h, const double*) { return h->a_val.p; }
+const float* a_values(psipm_handle* h, const float*) { return h->a_valf.p; }
+const double* weights(psipm_handle* h, const double*) { return h->w.p; }
+const float* weights(psipm_handle* h, const float*) { return h->wf.p; }
+
+template <typename T>
+PcgArgs<T> pcg_args(psipm_handle* h) {
+    const T* tag = nullptr;
+    PcgArgs<T> a;
+    a.sp = spmv_layout<T>(h);
+    a.at_val = at_values(h, tag);
+    a.a_val = a_values(h, tag);
+    a.w = weights(h, tag);
+    a.delta = (T)h->delta;
+    PrecLayout<T>& pc = a.pc;
     pc.m = (int)h->m;
+    FactorStore<T>& fs = fstore(h, tag);
     if (h->have_symbolic) {
         pc.perm = h->s_perm.p;
         pc.iperm = h->s_iperm.p;
-        pc.dscp = h->f64.dscp.p;
-        pc.G = h->f64.G.p;
+        pc.dscp = fs.dscp.p;
+        pc.G = fs.G.p;
         pc.panel_off = h->s_panel_off.p;
         pc.sn_first = h->s_first.p;
         pc.sn_rowptr = h->s_rowptr.p;
@@ -285,19 +309,19 @@ PcgArgs<double> pcg_args(psipm_handle* h) {
         pc.fwd_tasks = h->fwd_tasks_d.p;
         pc.bwd_ptr = h->bwd_ptr_d.p;
         pc.bwd_tasks = h->bwd_tasks_d.p;
-        pc.xp = h->f64.xp.p;
-        pc.yp = h->f64.yp.p;
-        pc.uvec = h->f64.uvec.p;
+        pc.xp = fs.xp.p;
+        pc.yp = fs.yp.p;
+        pc.uvec = fs.uvec.p;
         pc.fpre_ptr = h->fpre_ptr_d.p;
         pc.fpre_tasks = h->fpre_tasks_d.p;
         pc.bpre_ptr = h->bpre_ptr_d.p;
         pc.bpre_tasks = h->bpre_tasks_d.p;
-        pc.fvec = h->f64.fvec.p;
-        pc.bvec = h->f64.bvec.p;
-        pc.GT = h->f64.GT.p;
+        pc.fvec = fs.fvec.p;
+        pc.bvec = fs.bvec.p;
+        pc.GT = fs.GT.p;
         pc.gt_off = h->s_panel_off.p;
     }
-    PcgStore<double>& st = h->p64;
+    PcgStore<T>& st = pstore(h, tag);
     const int64_t m = h->m, n = h->n;
     st.x.reserve(m);
     st.r.reserve(m);
@@ -306,6 +330,7 @@ PcgArgs<double> pcg_args(psipm_handle* h) {
     st.q.reserve(m);
     st.t.reserve(n);
     st.tr.reserve(m);
+    st.rhs.reserve(m);
     st.chunk_part.reserve(std::max(1, h->n_chunks));
     h->part.reserve((size_t)2 * 4 * std::max(1, h->coop_blocks));
     h->ctrl.reserve(4);
@@ -326,7 +351,7 @@ PcgArgs<double> pcg_args(psipm_handle* h) {
     return a;
 }
 
-size_t pcg_smem() { return (size_t)kPcgWarps * kStageChunk * sizeof(double); }
+size_t pcg_smem() { return (size_t)kPcgWarps * kStageChunk * sizeof(double); }  // covers float too
 
 void launch_coop(psipm_handle* h, const void* fn, void** args) {
     dim3 grid(h->coop_blocks), block(kPcgThreads);
@@ -448,9 +473,7 @@ void analyse(psipm_handle* h) {
     h->bpre_ptr_d.upload(h->bpre_ptr, st);
     h->fpre_tasks_d.upload(fp, st);
     h->bpre_tasks_d.upload(bp, st);
-    h->f64.GT.reserve(std::max<int64_t>(1, s.panel_total));
-    h->f64.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
-    h->f64.bvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
+    // per level: fronts factored one per CTA (small) or by the multi-CTA path (big)
     h->small_ptr.assign(s.nlevels + 1, 0);
     h->big_ptr.assign(s.nlevels + 1, 0);
     h->small_sn.clear();
@@ -472,16 +495,27 @@ void analyse(psipm_handle* h) {
     h->bwd_ptr_d.upload(h->bwd_ptr, st);
     h->fwd_tasks_d.upload(ft, st);
     h->bwd_tasks_d.upload(bt, st);
-    // numeric storage
+    // numeric storage (entries are assembled in FP64, the factor lives in the
+    // handle's precision)
     h->pval.reserve(std::max<int64_t>(1, s.nentries));
-    h->f64.ms.reserve(std::max<int64_t>(1, s.nentries));
-    h->f64.G.reserve(std::max<int64_t>(1, s.panel_total));
-    h->f64.update.reserve(std::max<int64_t>(1, s.update_total));
-    h->f64.front.reserve(std::max<int64_t>(1, fmax_total));
-    h->f64.xp.reserve(h->m);
-    h->f64.yp.reserve(h->m);
-    h->f64.uvec.reserve(std::max<int64_t>(1, s.uvec_total));
-    h->f64.dscp.reserve(h->m);
+    auto reserve_factor = [&](auto& fs) {
+        fs.ms.reserve(std::max<int64_t>(1, s.nentries));
+        fs.G.reserve(std::max<int64_t>(1, s.panel_total));
+        fs.GT.reserve(std::max<int64_t>(1, s.panel_total));
+        fs.update.reserve(std::max<int64_t>(1, s.update_total));
+        fs.front.reserve(std::max<int64_t>(1, fmax_total));
+        fs.xp.reserve(h->m);
+        fs.yp.reserve(h->m);
+        fs.uvec.reserve(std::max<int64_t>(1, s.uvec_total));
+        fs.dscp.reserve(h->m);
+        fs.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
+        fs.bvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
+    };
+    if (h->precision == PSIPM_FP32_REFINED)
+        reserve_factor(h->f32);
+    else
+        reserve_factor(h->f64);
+    h->dscp64.reserve(h->m);
     h->fail.reserve(1);
     PSIPM_CUDA(cudaStreamSynchronize(st));
     h->have_symbolic = true;
@@ -499,6 +533,10 @@ void compute_weights(psipm_handle* h) {
     LAUNCH(h, k_weights<<<blocks_for(n, 256), 256, 0, h->stream>>>(n, h->theta.p, h->w.p));
     LAUNCH(h, k_diag_full<<<blocks_for(m, 256), 256, 0, h->stream>>>(
                   (int)m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->w.p, h->diag_full.p));
+    if (h->precision == PSIPM_FP32_REFINED) {
+        h->wf.reserve(n);
+        LAUNCH(h, k_cast<float><<<blocks_for(n, 256), 256, 0, h->stream>>>(n, h->w.p, h->wf.p));
+    }
 }
 
 
@@ -543,6 +581,64 @@ void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
     LAUNCH(h, k_g_trsm<T><<<blocks_for(r, 32), 256, 0, st>>>(F, r, c, fa.G + s.panel_off[sn]));
     dim3 tgrid((c + 31) / 32, (r + 31) / 32), tblock(32, 8);
     LAUNCH(h, k_transpose_panel<T><<<tgrid, tblock, 0, st>>>(fa.G + s.panel_off[sn], r, c, fa.GT + s.panel_off[sn]));
+}
+
+
+// F1 in FP64 (bit-reproducible entries and Jacobi scale), then the factor in
+// precision T with the shift ladder; returns the shift index used or -1.
+template <typename T>
+int factor_numeric(psipm_handle* h, double delta, int start_shift) {
+    const T* tag = nullptr;
+    Symbolic& s = h->sym;
+    cudaStream_t st = h->stream;
+    FactorStore<T>& fs = fstore(h, tag);
+    if (s.nentries)
+        LAUNCH(h, k_assemble_entries<<<blocks_for(s.nentries, 256), 256, 0, st>>>(
+                      s.nentries, h->s_ent_ptr.p, h->s_contrib_col.p, h->s_contrib_val.p, h->d_core.p, h->w.p,
+                      h->pval.p));
+    LAUNCH(h, k_diag_fix<<<blocks_for(h->m, 256), 256, 0, st>>>((int)h->m, h->s_diag_entry.p, h->s_perm.p,
+                                                                 h->diag_full.p, delta, h->pval.p, h->dscp64.p));
+    if (s.nentries)
+        LAUNCH(h, k_scale_entries<T><<<blocks_for(s.nentries, 256), 256, 0, st>>>(
+                      s.nentries, h->s_ent_row.p, h->s_ent_colg.p, h->pval.p, h->dscp64.p, fs.ms.p));
+    LAUNCH(h, k_cast<T><<<blocks_for(h->m, 256), 256, 0, st>>>(h->m, h->dscp64.p, fs.dscp.p));
+    FactorArgs<T> fa;
+    fa.sn_first = h->s_first.p;
+    fa.sn_rowptr = h->s_rowptr.p;
+    fa.panel_off = h->s_panel_off.p;
+    fa.update_off = h->s_update_off.p;
+    fa.uvec_off = h->s_uvec_off.p;
+    fa.child_ptr = h->s_child_ptr.p;
+    fa.child_list = h->s_child_list.p;
+    fa.relind = h->s_relind.p;
+    fa.sn_entptr = h->s_entptr.p;
+    fa.ent_col = h->s_ent_col.p;
+    fa.ent_rowpos = h->s_ent_rowpos.p;
+    fa.ms = fs.ms.p;
+    fa.G = fs.G.p;
+    fa.GT = fs.GT.p;
+    fa.update = fs.update.p;
+    fa.front = fs.front.p;
+    fa.front_off = h->s_front_off.p;
+    fa.fail = h->fail.p;
+    require((int)h->small_ptr.size() == s.nlevels + 1 && (int)h->big_ptr.size() == s.nlevels + 1 &&
+                h->small_ptr[s.nlevels] + h->big_ptr[s.nlevels] == s.ns,
+            PSIPM_ERR_STATE, "level tables do not match the symbolic factor");
+    for (int k = start_shift; k < 8; ++k) {
+        fa.eta = kShifts[k];
+        PSIPM_CUDA(cudaMemsetAsync(h->fail.p, 0, sizeof(int), st));
+        for (int l = 0; l < s.nlevels; ++l) {
+            int cnt = h->small_ptr[l + 1] - h->small_ptr[l];
+            if (cnt)
+                LAUNCH(h, k_factor_level<T><<<cnt, kFactorThreads, 0, st>>>(fa, h->small_sn_d.p + h->small_ptr[l]));
+            for (int q = h->big_ptr[l]; q < h->big_ptr[l + 1]; ++q) factor_big_front<T>(h, h->big_sn[q], fa);
+        }
+        int failed = 0;
+        PSIPM_CUDA(cudaMemcpyAsync(&failed, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        if (!failed) return k;
+    }
+    return -1;
 }
 
 // ---------------------------------------------------------------------------
@@ -637,10 +733,11 @@ void set_core_internal(psipm_handle* h, std::vector<int64_t> newcore) {
     h->core_flags.upload(f, h->stream);
 }
 
-void run_pcg(psipm_handle* h, const double* rhs_dev, double tol, int maxit, int variant, int replacement,
+template <typename T>
+void run_pcg(psipm_handle* h, const T* rhs_dev, double tol, int maxit, int variant, int replacement,
              double gap_tol, psipm_pcg_info* info) {
     require(h->have_factor, PSIPM_ERR_STATE, "pcg before a successful factor");
-    PcgArgs<double> a = pcg_args(h);
+    PcgArgs<T> a = pcg_args<T>(h);
     a.rhs = rhs_dev;
     a.variant = variant;
     a.maxit = maxit;
@@ -656,7 +753,7 @@ void run_pcg(psipm_handle* h, const double* rhs_dev, double tol, int maxit, int 
     PSIPM_CUDA(cudaMemsetAsync(h->ctrl.p, 0, 4 * sizeof(int), h->stream));
     void* args[] = {&a};
     PSIPM_CUDA(cudaEventRecord(h->ev0, h->stream));
-    launch_coop(h, (const void*)k_pcg<double>, args);
+    launch_coop(h, (const void*)k_pcg<T>, args);
     PSIPM_CUDA(cudaEventRecord(h->ev1, h->stream));
     int io[16];
     double dd[8];
@@ -682,10 +779,20 @@ void run_pcg(psipm_handle* h, const double* rhs_dev, double tol, int maxit, int 
     }
 }
 
+__global__ void k_widen(long long n, const float* __restrict__ in, double* __restrict__ out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)in[i];
+}
+
 void copy_out(psipm_handle* h, double* host, const double* dev, int64_t n) {
     if (host && n) PSIPM_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
 }
 
+}  // namespace
+
+namespace {
+const double* solve_normal(psipm_handle* h, const double* rhs, double tol, int maxit, int variant, int replacement,
+                           double gap_tol, psipm_pcg_info* info);
 }  // namespace
 
 // ===========================================================================
@@ -733,6 +840,14 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
                                         (int)pcg_smem()));
         PSIPM_CUDA(cudaFuncSetAttribute(k_apply<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)pcg_smem()));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)pcg_smem()));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)pcg_smem()));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_trsm_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kNB * (kNB + 1) * sizeof(float))));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kNB * (kNB + 1) * sizeof(float))));
         PSIPM_CUDA(cudaFuncSetAttribute(k_trsm_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)(2 * kNB * (kNB + 1) * sizeof(double))));
         PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -745,7 +860,9 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
                                                                  pcg_smem()));
         int per_sm3 = 0;
         PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_matvec<double>, kPcgThreads, 0));
-        per_sm = std::min(std::min(per_sm, per_sm2), per_sm3);
+        int per_sm4 = 0;
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, k_pcg<float>, kPcgThreads, pcg_smem()));
+        per_sm = std::min(std::min(std::min(per_sm, per_sm2), per_sm3), per_sm4);
         require(per_sm >= 1, PSIPM_ERR_UNSUPPORTED, "PCG kernel does not fit on an SM");
         // blocks per SM of the persistent kernels (PSIPM_BLOCKS_PER_SM overrides)
         int want = 4;
@@ -931,53 +1048,8 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
         Symbolic& s = h->sym;
         cudaStream_t st = h->stream;
         PSIPM_CUDA(cudaEventRecord(h->ev0, st));
-        if (s.nentries)
-            LAUNCH(h, k_assemble_entries<<<blocks_for(s.nentries, 256), 256, 0, st>>>(
-                          s.nentries, h->s_ent_ptr.p, h->s_contrib_col.p, h->s_contrib_val.p, h->d_core.p,
-                          h->w.p, h->pval.p));
-        LAUNCH(h, k_diag_fix<<<blocks_for(h->m, 256), 256, 0, st>>>((int)h->m, h->s_diag_entry.p, h->s_perm.p,
-                                                                     h->diag_full.p, delta, h->pval.p,
-                                                                     h->f64.dscp.p));
-        if (s.nentries)
-            LAUNCH(h, k_scale_entries<double><<<blocks_for(s.nentries, 256), 256, 0, st>>>(
-                          s.nentries, h->s_ent_row.p, h->s_ent_colg.p, h->pval.p, h->f64.dscp.p, h->f64.ms.p));
-        FactorArgs<double> fa;
-        fa.sn_first = h->s_first.p;
-        fa.sn_rowptr = h->s_rowptr.p;
-        fa.panel_off = h->s_panel_off.p;
-        fa.update_off = h->s_update_off.p;
-        fa.uvec_off = h->s_uvec_off.p;
-        fa.child_ptr = h->s_child_ptr.p;
-        fa.child_list = h->s_child_list.p;
-        fa.relind = h->s_relind.p;
-        fa.sn_entptr = h->s_entptr.p;
-        fa.ent_col = h->s_ent_col.p;
-        fa.ent_rowpos = h->s_ent_rowpos.p;
-        fa.ms = h->f64.ms.p;
-        fa.G = h->f64.G.p;
-        fa.GT = h->f64.GT.p;
-        fa.update = h->f64.update.p;
-        fa.front = h->f64.front.p;
-        fa.front_off = h->s_front_off.p;
-        fa.fail = h->fail.p;
-        int used = -1;
-        for (int k = start_shift; k < 8; ++k) {
-            fa.eta = kShifts[k];
-            PSIPM_CUDA(cudaMemsetAsync(h->fail.p, 0, sizeof(int), st));
-            for (int l = 0; l < s.nlevels; ++l) {
-                int cnt = h->small_ptr[l + 1] - h->small_ptr[l];
-                if (cnt)
-                    LAUNCH(h, k_factor_level<double><<<cnt, kFactorThreads, 0, st>>>(fa, h->small_sn_d.p + h->small_ptr[l]));
-                for (int q = h->big_ptr[l]; q < h->big_ptr[l + 1]; ++q) factor_big_front<double>(h, h->big_sn[q], fa);
-            }
-            int failed = 0;
-            PSIPM_CUDA(cudaMemcpyAsync(&failed, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-            PSIPM_CUDA(cudaStreamSynchronize(st));
-            if (!failed) {
-                used = k;
-                break;
-            }
-        }
+        int used = h->precision == PSIPM_FP32_REFINED ? factor_numeric<float>(h, delta, start_shift)
+                                                      : factor_numeric<double>(h, delta, start_shift);
         PSIPM_CUDA(cudaEventRecord(h->ev1, st));
         PSIPM_CUDA(cudaEventSynchronize(h->ev1));
         float ms = 0.f;
@@ -1008,13 +1080,24 @@ int psipm_apply(psipm_handle* h, const double* r, double* z) {
     if (!r || !z) return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
         require(h->have_factor, PSIPM_ERR_STATE, "apply before a successful factor");
-        PcgArgs<double> a = pcg_args(h);
         h->r1.upload(r, h->m, h->stream);
         h->r2.reserve(h->m);
-        const double* in = h->r1.p;
-        double* outp = h->r2.p;
-        void* args[] = {&a, (void*)&in, (void*)&outp};
-        launch_coop(h, (const void*)k_apply<double>, args);
+        if (h->precision == PSIPM_FP32_REFINED) {
+            PcgArgs<float> a = pcg_args<float>(h);
+            PcgStore<float>& st = h->p32;
+            LAUNCH(h, k_cast<float><<<blocks_for(h->m, 256), 256, 0, h->stream>>>(h->m, h->r1.p, st.rhs.p));
+            const float* in = st.rhs.p;
+            float* outp = st.tr.p;
+            void* args[] = {&a, (void*)&in, (void*)&outp};
+            launch_coop(h, (const void*)k_apply<float>, args);
+            LAUNCH(h, k_widen<<<blocks_for(h->m, 256), 256, 0, h->stream>>>(h->m, st.tr.p, h->r2.p));
+        } else {
+            PcgArgs<double> a = pcg_args<double>(h);
+            const double* in = h->r1.p;
+            double* outp = h->r2.p;
+            void* args[] = {&a, (void*)&in, (void*)&outp};
+            launch_coop(h, (const void*)k_apply<double>, args);
+        }
         copy_out(h, z, h->r2.p, h->m);
     });
 }
@@ -1023,7 +1106,7 @@ int psipm_matvec(psipm_handle* h, const double* v, double* y) {
     if (!v || !y) return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
         require(h->have_theta, PSIPM_ERR_STATE, "matvec before set_theta");
-        PcgArgs<double> a = pcg_args(h);
+        PcgArgs<double> a = pcg_args<double>(h);  // the operator is always applied in FP64 here
         PSIPM_CUDA(cudaMemcpyAsync(h->p64.p.p, v, h->m * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         void* args[] = {&a};
         launch_coop(h, (const void*)k_matvec<double>, args);
@@ -1037,11 +1120,11 @@ int psipm_pcg(psipm_handle* h, const double* rhs, double tol, int32_t maxit, int
     if (!rhs || !x || maxit < 0 || (variant != PSIPM_PCG_SPECTRAL && variant != PSIPM_PCG_HSD))
         return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
-        h->p64.rhs.upload(rhs, h->m, h->stream);
+        h->rhs64.upload(rhs, h->m, h->stream);
         psipm_pcg_info local;
-        run_pcg(h, h->p64.rhs.p, tol, maxit, variant, replacement, gap_tolerance, &local);
-        copy_out(h, x, h->p64.x.p, h->m);
-        copy_out(h, residual, h->p64.tr.p, h->m);
+        const double* xd = solve_normal(h, h->rhs64.p, tol, maxit, variant, replacement, gap_tolerance, &local);
+        copy_out(h, x, xd, h->m);
+        if (residual) copy_out(h, residual, h->r64.p, h->m);
         copy_out(h, alphas, h->alphas.p, local.n_alpha);
         copy_out(h, betas, h->betas.p, local.n_beta);
         copy_out(h, history, h->history.p, local.n_history);
@@ -1083,18 +1166,148 @@ __global__ void k_dx(long long n, const int* __restrict__ ptr, const int* __rest
     dx[j] = wr1[j] + s / theta[j];
 }
 
+// t = w o (A^T x)  (FP64, one thread per column)
+__global__ void k_at_w(long long n, const int* __restrict__ ptr, const int* __restrict__ idx,
+                       const double* __restrict__ val, const double* __restrict__ w, const double* __restrict__ x,
+                       double* __restrict__ t) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double s = 0.0;
+    for (int k = ptr[j]; k < ptr[j + 1]; ++k) s += val[k] * x[idx[k]];
+    t[j] = w[j] * s;
+}
+
+// r = rhs - (A t + delta x)   (FP64, one warp per row); norm2 += r.r
+__global__ void k_residual(long long m, const int* __restrict__ ptr, const int* __restrict__ idx,
+                           const double* __restrict__ val, const double* __restrict__ t, double delta,
+                           const double* __restrict__ x, const double* __restrict__ rhs, double* __restrict__ r,
+                           double* __restrict__ norm2) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    double acc = 0.0;
+    for (long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
+        double s = 0.0;
+        for (int k = ptr[i] + lane; k < ptr[i + 1]; k += 32) s += val[k] * t[idx[k]];
+        s = warp_sum(s);
+        if (lane == 0) {
+            const double ri = rhs[i] - (s + delta * x[i]);
+            r[i] = ri;
+            acc += ri * ri;
+        }
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) atomicAdd(norm2, acc);
+}
+
+__global__ void k_scale_narrow(long long m, const double* __restrict__ r, double s, float* __restrict__ out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < m) out[i] = (float)(r[i] * s);
+}
+
+__global__ void k_axpy_widen(long long m, double a, const float* __restrict__ d, double* __restrict__ x) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < m) x[i] += a * (double)d[i];
+}
+
+// r64 = rhs64 - H x64 in FP64; returns ||r64||
+double fp64_residual(psipm_handle* h, const double* rhs, const double* x) {
+    const int64_t m = h->m, n = h->n;
+    cudaStream_t st = h->stream;
+    h->t64.reserve(n);
+    h->r64.reserve(m);
+    h->norm64.reserve(1);
+    PSIPM_CUDA(cudaMemsetAsync(h->norm64.p, 0, sizeof(double), st));
+    LAUNCH(h, k_at_w<<<blocks_for(n, 256), 256, 0, st>>>(n, h->at_ptr.p, h->at_idx.p, h->at_val.p, h->w.p, x,
+                                                          h->t64.p));
+    const int rows = (int)std::min<int64_t>(blocks_for(m * 32, 256), 8 * std::max(1, h->num_sms));
+    LAUNCH(h, k_residual<<<rows, 256, 0, st>>>(m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->t64.p, h->delta, x, rhs,
+                                               h->r64.p, h->norm64.p));
+    double nrm2 = 0.0;
+    PSIPM_CUDA(cudaMemcpyAsync(&nrm2, h->norm64.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    PSIPM_CUDA(cudaStreamSynchronize(st));
+    return std::sqrt(nrm2);
+}
+
+// Solve H x = rhs (rhs FP64 on the device) to relative residual tol.
+// FP64 mode: one persistent PCG.  FP32_REFINED: iterative refinement in FP64
+// around FP32 persistent PCG sweeps on the normalised residual:
+//   x = 0; repeat { r = rhs - H x (FP64); stop if |r|/scale <= tol;
+//                   d = PCG32(r/|r|, tol_in); x += |r| d }
+// Returns the device pointer of x (FP64).
+const double* solve_normal(psipm_handle* h, const double* rhs, double tol, int maxit, int variant, int replacement,
+                           double gap_tol, psipm_pcg_info* info) {
+    require(h->have_factor, PSIPM_ERR_STATE, "solve before a successful factor");
+    if (h->precision != PSIPM_FP32_REFINED) {
+        run_pcg<double>(h, rhs, tol, maxit, variant, replacement, gap_tol, info);
+        h->r64.reserve(h->m);
+        PSIPM_CUDA(cudaMemcpyAsync(h->r64.p, h->p64.tr.p, h->m * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        return h->p64.x.p;
+    }
+    const int64_t m = h->m;
+    cudaStream_t st = h->stream;
+    h->x64.zero(m, st);
+    PcgStore<float>& s32 = h->p32;
+    pcg_args<float>(h);  // sizes the FP32 work vectors
+    double rnorm = fp64_residual(h, rhs, h->x64.p);
+    const double rhs_norm = rnorm;
+    const double scale = variant == PSIPM_PCG_HSD ? rhs_norm : std::max(1.0, rhs_norm);
+    const double target = variant == PSIPM_PCG_HSD ? std::max(tol * rhs_norm, 64.0 * 2.220446049250313e-16 * rhs_norm)
+                                                   : tol * scale;
+    psipm_pcg_info total;
+    std::memset(&total, 0, sizeof(total));
+    psipm_pcg_info first;
+    std::memset(&first, 0, sizeof(first));
+    int sweeps = 0;
+    int last_info = 0;
+    const int max_sweeps = 8;
+    int budget = maxit;
+    while (rnorm > target && sweeps < max_sweeps && budget > 0 && rnorm > 0.0) {
+        LAUNCH(h, k_scale_narrow<<<blocks_for(m, 256), 256, 0, st>>>(m, h->r64.p, 1.0 / rnorm, s32.rhs.p));
+        const double inner = std::min(0.5, std::max(1e-5, 0.5 * target / rnorm));
+        psipm_pcg_info one;
+        run_pcg<float>(h, s32.rhs.p, inner, budget, variant, replacement, gap_tol, &one);
+        if (sweeps == 0) first = one;
+        last_info = one.info;
+        total.iterations += one.iterations;
+        total.matvecs += one.matvecs + 1;
+        total.replacements += one.replacements;
+        total.residual_checks += one.residual_checks + 1;
+        total.seconds += one.seconds;
+        for (int q = 0; q < 4; ++q) total.phase_seconds[q] += one.phase_seconds[q];
+        budget -= std::max(1, one.iterations);
+        LAUNCH(h, k_axpy_widen<<<blocks_for(m, 256), 256, 0, st>>>(m, rnorm, s32.x.p, h->x64.p));
+        rnorm = fp64_residual(h, rhs, h->x64.p);
+        ++sweeps;
+        if (one.iterations == 0 && one.info != 0) break;  // no progress possible
+        if (!std::isfinite(rnorm)) break;
+    }
+    if (info) {
+        *info = total;
+        info->n_alpha = first.n_alpha;  // Lanczos data of the first (longest) sweep
+        info->n_beta = first.n_beta;
+        info->n_history = first.n_history;
+        info->refinements = sweeps;
+        info->relative_residual = scale > 0.0 ? rnorm / scale : 0.0;
+        const bool converged = rnorm <= target;
+        info->ok = converged ? 1 : 0;
+        info->info = converged ? 0 : (last_info != 0 ? last_info : maxit);
+    }
+    return h->x64.p;
+}
+
 void solve_device(psipm_handle* h, const double* r1d, const double* r2d, double tol, int maxit, int variant,
-                  int replacement, double gap_tol, double* dxd, psipm_pcg_info* info) {
+                  int replacement, double gap_tol, double* dxd, psipm_pcg_info* info, const double** dy_out) {
     const int64_t m = h->m, n = h->n;
     cudaStream_t st = h->stream;
     h->wr1.reserve(n);
-    h->p64.rhs.reserve(m);
+    h->rhs64.reserve(m);
     LAUNCH(h, k_div<<<blocks_for(n, 256), 256, 0, st>>>(n, r1d, h->theta.p, h->wr1.p));
     LAUNCH(h, k_rhs<<<blocks_for(m, 256), 256, 0, st>>>((int)m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->wr1.p,
-                                                         r2d, h->p64.rhs.p));
-    run_pcg(h, h->p64.rhs.p, tol, maxit, variant, replacement, gap_tol, info);
-    LAUNCH(h, k_dx<<<blocks_for(n, 256), 256, 0, st>>>(n, h->at_ptr.p, h->at_idx.p, h->at_val.p, h->p64.x.p,
-                                                        h->wr1.p, h->theta.p, dxd));
+                                                         r2d, h->rhs64.p));
+    const double* dy = solve_normal(h, h->rhs64.p, tol, maxit, variant, replacement, gap_tol, info);
+    LAUNCH(h, k_dx<<<blocks_for(n, 256), 256, 0, st>>>(n, h->at_ptr.p, h->at_idx.p, h->at_val.p, dy, h->wr1.p,
+                                                        h->theta.p, dxd));
+    *dy_out = dy;
 }
 
 }  // namespace
@@ -1111,10 +1324,11 @@ int psipm_solve(psipm_handle* h, const double* r1, const double* r2, double tol,
         h->r2.upload(r2, h->m, h->stream);
         h->dx.reserve(h->n);
         psipm_pcg_info local;
-        solve_device(h, h->r1.p, h->r2.p, tol, maxit, variant, replacement, gap_tolerance, h->dx.p, &local);
+        const double* dyd = nullptr;
+        solve_device(h, h->r1.p, h->r2.p, tol, maxit, variant, replacement, gap_tolerance, h->dx.p, &local, &dyd);
         copy_out(h, dx, h->dx.p, h->n);
-        copy_out(h, dy, h->p64.x.p, h->m);
-        copy_out(h, residual, h->p64.tr.p, h->m);
+        copy_out(h, dy, dyd, h->m);
+        if (residual) copy_out(h, residual, h->r64.p, h->m);
         copy_out(h, alphas, h->alphas.p, local.n_alpha);
         copy_out(h, betas, h->betas.p, local.n_beta);
         copy_out(h, history, h->history.p, local.n_history);
@@ -1128,8 +1342,9 @@ int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev,
     if (!r1_dev || !r2_dev || !dx_dev || !dy_dev || maxit < 0) return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
         require(h->have_factor, PSIPM_ERR_STATE, "solve before a successful factor");
-        solve_device(h, r1_dev, r2_dev, tol, maxit, variant, replacement, gap_tolerance, dx_dev, info);
-        PSIPM_CUDA(cudaMemcpyAsync(dy_dev, h->p64.x.p, h->m * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        const double* dyd = nullptr;
+        solve_device(h, r1_dev, r2_dev, tol, maxit, variant, replacement, gap_tolerance, dx_dev, info, &dyd);
+        PSIPM_CUDA(cudaMemcpyAsync(dy_dev, dyd, h->m * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     });
 }
 
@@ -1140,7 +1355,8 @@ int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t
     if (!r || !z || !stamps || cap <= 0 || !count) return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
         require(h->have_factor, PSIPM_ERR_STATE, "apply before a successful factor");
-        PcgArgs<double> a = pcg_args(h);
+        require(h->precision == PSIPM_FP64, PSIPM_ERR_UNSUPPORTED, "apply trace is FP64 only");
+        PcgArgs<double> a = pcg_args<double>(h);
         DevBuf<long long> tr;
         tr.zero(cap, h->stream);
         a.pc.trace = tr.p;

@@ -229,6 +229,7 @@ class GpuStableActiveColumnPreconditioner:
         self.pcg_replacements = 0
         self.pcg_bytes = 0.0  # algorithmic bytes of all PCG launches (roofline numerator)
         self.pcg_phase_seconds = np.zeros(4)  # H·p, updates, applies, other (device clock)
+        self.refinement_sweeps = 0  # FP64 refinement sweeps around FP32 PCG (FP32_REFINED)
         # host<->device traffic through the C ABI (bytes)
         self.h2d_bytes = 0
         self.d2h_bytes = 0
@@ -516,8 +517,10 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self.pcg_matvecs += res.matvecs
         self.pcg_replacements += res.replacements
         self.pcg_phase_seconds += np.asarray(res.phase_seconds)
+        bv = 4 if self.precision == _lib.FP32_REFINED else 8
         self.pcg_bytes += pcg_launch_bytes(self.m, self.n, self.A.nnz, self.nnz_factor, res.iterations,
-                                           res.matvecs, res.iterations + 2 + res.replacements)
+                                           res.matvecs, res.iterations + 2 + res.replacements, bv)
+        self.refinement_sweeps += res.refinements
         self.h2d_bytes += 8 * (self.n + self.m)
         self.d2h_bytes += 8 * (self.n + self.m)
         return dx, KrylovResult(res.x, res.info, res.iterations, res.relative_residual, float(cond),
