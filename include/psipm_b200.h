@@ -45,8 +45,12 @@ typedef struct psipm_handle psipm_handle;
 #define PSIPM_PCG_HSD 1      /* psipm_v3_1_hsd.py:1015-1063 */
 
 /* precision of the PCG inner iterations */
-#define PSIPM_FP64 0       /* everything in FP64 */
-#define PSIPM_FP32_REFINED 1 /* FP32 SpMV/factor/solves, FP64 true residual + refinement */
+#define PSIPM_FP64 0         /* everything in FP64 */
+#define PSIPM_FP32_REFINED 1 /* FP32 SpMV/factor/solves inside FP64 refinement sweeps; when a sweep
+                                stops reducing the FP64 residual the solve finishes with FP64 PCG
+                                around the FP32 preconditioner */
+#define PSIPM_FP32_PRECOND 2 /* FP64 PCG (operator, vectors) with the preconditioner's factor and
+                                triangular solves in FP32 */
 
 typedef struct {
     int32_t info;            /* reference KrylovResult.info: 0 ok, >0 limit, -1..-7 breakdown */

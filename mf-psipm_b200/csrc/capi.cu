@@ -280,18 +280,19 @@ const float* a_values(psipm_handle* h, const float*) { return h->a_valf.p; }
 const double* weights(psipm_handle* h, const double*) { return h->w.p; }
 const float* weights(psipm_handle* h, const float*) { return h->wf.p; }
 
-template <typename T>
-PcgArgs<T> pcg_args(psipm_handle* h) {
+template <typename T, typename P = T>
+PcgArgs<T, P> pcg_args(psipm_handle* h) {
     const T* tag = nullptr;
-    PcgArgs<T> a;
+    const P* ptag = nullptr;
+    PcgArgs<T, P> a;
     a.sp = spmv_layout<T>(h);
     a.at_val = at_values(h, tag);
     a.a_val = a_values(h, tag);
     a.w = weights(h, tag);
     a.delta = (T)h->delta;
-    PrecLayout<T>& pc = a.pc;
+    PrecLayout<P>& pc = a.pc;
     pc.m = (int)h->m;
-    FactorStore<T>& fs = fstore(h, tag);
+    FactorStore<P>& fs = fstore(h, ptag);
     if (h->have_symbolic) {
         pc.perm = h->s_perm.p;
         pc.iperm = h->s_iperm.p;
@@ -511,7 +512,7 @@ void analyse(psipm_handle* h) {
         fs.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
         fs.bvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
     };
-    if (h->precision == PSIPM_FP32_REFINED)
+    if (h->precision != PSIPM_FP64)
         reserve_factor(h->f32);
     else
         reserve_factor(h->f64);
@@ -733,11 +734,11 @@ void set_core_internal(psipm_handle* h, std::vector<int64_t> newcore) {
     h->core_flags.upload(f, h->stream);
 }
 
-template <typename T>
+template <typename T, typename P = T>
 void run_pcg(psipm_handle* h, const T* rhs_dev, double tol, int maxit, int variant, int replacement,
              double gap_tol, psipm_pcg_info* info) {
     require(h->have_factor, PSIPM_ERR_STATE, "pcg before a successful factor");
-    PcgArgs<T> a = pcg_args<T>(h);
+    PcgArgs<T, P> a = pcg_args<T, P>(h);
     a.rhs = rhs_dev;
     a.variant = variant;
     a.maxit = maxit;
@@ -753,7 +754,7 @@ void run_pcg(psipm_handle* h, const T* rhs_dev, double tol, int maxit, int varia
     PSIPM_CUDA(cudaMemsetAsync(h->ctrl.p, 0, 4 * sizeof(int), h->stream));
     void* args[] = {&a};
     PSIPM_CUDA(cudaEventRecord(h->ev0, h->stream));
-    launch_coop(h, (const void*)k_pcg<T>, args);
+    launch_coop(h, (const void*)k_pcg<T, P>, args);
     PSIPM_CUDA(cudaEventRecord(h->ev1, h->stream));
     int io[16];
     double dd[8];
@@ -779,11 +780,6 @@ void run_pcg(psipm_handle* h, const T* rhs_dev, double tol, int maxit, int varia
     }
 }
 
-__global__ void k_widen(long long n, const float* __restrict__ in, double* __restrict__ out) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) out[i] = (double)in[i];
-}
-
 void copy_out(psipm_handle* h, double* host, const double* dev, int64_t n) {
     if (host && n) PSIPM_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
 }
@@ -803,7 +799,8 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
     if (!out || m <= 0 || n < 0 || nnz < 0 || !colptr || (nnz && (!rowidx || !values)))
         return PSIPM_ERR_ARGUMENT;
     if (m >= (1ll << 31) || n >= (1ll << 31) || nnz >= (1ll << 31)) return PSIPM_ERR_UNSUPPORTED;
-    if (precision != PSIPM_FP64 && precision != PSIPM_FP32_REFINED) return PSIPM_ERR_ARGUMENT;
+    if (precision != PSIPM_FP64 && precision != PSIPM_FP32_REFINED && precision != PSIPM_FP32_PRECOND)
+        return PSIPM_ERR_ARGUMENT;
     *out = nullptr;
     if (colptr[0] != 0 || colptr[n] != nnz) return PSIPM_ERR_ARGUMENT;
     for (int64_t j = 0; j < n; ++j) {
@@ -836,13 +833,15 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
         PSIPM_CUDA(cudaGetDeviceProperties(&prop, device));
         h->num_sms = prop.multiProcessorCount;
         require(prop.cooperativeLaunch, PSIPM_ERR_UNSUPPORTED, "device lacks cooperative launch");
-        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)pcg_smem()));
-        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)pcg_smem()));
-        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)pcg_smem()));
-        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)pcg_smem()));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)pcg_smem()));
         PSIPM_CUDA(cudaFuncSetAttribute(k_trsm_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)(2 * kNB * (kNB + 1) * sizeof(float))));
@@ -853,16 +852,18 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
         PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)(2 * kNB * (kNB + 1) * sizeof(double))));
         int per_sm = 0;
-        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double>, kPcgThreads,
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double, double>, kPcgThreads,
                                                                  pcg_smem()));
         int per_sm2 = 0;
-        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_apply<double>, kPcgThreads,
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_apply<double, double>, kPcgThreads,
                                                                  pcg_smem()));
         int per_sm3 = 0;
-        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_matvec<double>, kPcgThreads, 0));
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_matvec<double, double>, kPcgThreads, 0));
         int per_sm4 = 0;
-        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, k_pcg<float>, kPcgThreads, pcg_smem()));
-        per_sm = std::min(std::min(std::min(per_sm, per_sm2), per_sm3), per_sm4);
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, k_pcg<float, float>, kPcgThreads, pcg_smem()));
+        int per_sm5 = 0;
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm5, k_pcg<double, float>, kPcgThreads, pcg_smem()));
+        per_sm = std::min(std::min(std::min(per_sm, per_sm2), std::min(per_sm3, per_sm4)), per_sm5);
         require(per_sm >= 1, PSIPM_ERR_UNSUPPORTED, "PCG kernel does not fit on an SM");
         // blocks per SM of the persistent kernels (PSIPM_BLOCKS_PER_SM overrides)
         int want = 4;
@@ -1048,7 +1049,7 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
         Symbolic& s = h->sym;
         cudaStream_t st = h->stream;
         PSIPM_CUDA(cudaEventRecord(h->ev0, st));
-        int used = h->precision == PSIPM_FP32_REFINED ? factor_numeric<float>(h, delta, start_shift)
+        int used = h->precision != PSIPM_FP64 ? factor_numeric<float>(h, delta, start_shift)
                                                       : factor_numeric<double>(h, delta, start_shift);
         PSIPM_CUDA(cudaEventRecord(h->ev1, st));
         PSIPM_CUDA(cudaEventSynchronize(h->ev1));
@@ -1082,21 +1083,18 @@ int psipm_apply(psipm_handle* h, const double* r, double* z) {
         require(h->have_factor, PSIPM_ERR_STATE, "apply before a successful factor");
         h->r1.upload(r, h->m, h->stream);
         h->r2.reserve(h->m);
-        if (h->precision == PSIPM_FP32_REFINED) {
-            PcgArgs<float> a = pcg_args<float>(h);
-            PcgStore<float>& st = h->p32;
-            LAUNCH(h, k_cast<float><<<blocks_for(h->m, 256), 256, 0, h->stream>>>(h->m, h->r1.p, st.rhs.p));
-            const float* in = st.rhs.p;
-            float* outp = st.tr.p;
-            void* args[] = {&a, (void*)&in, (void*)&outp};
-            launch_coop(h, (const void*)k_apply<float>, args);
-            LAUNCH(h, k_widen<<<blocks_for(h->m, 256), 256, 0, h->stream>>>(h->m, st.tr.p, h->r2.p));
-        } else {
-            PcgArgs<double> a = pcg_args<double>(h);
+        if (h->precision != PSIPM_FP64) {
+            PcgArgs<double, float> a = pcg_args<double, float>(h);
             const double* in = h->r1.p;
             double* outp = h->r2.p;
             void* args[] = {&a, (void*)&in, (void*)&outp};
-            launch_coop(h, (const void*)k_apply<double>, args);
+            launch_coop(h, (const void*)k_apply<double, float>, args);
+        } else {
+            PcgArgs<double, double> a = pcg_args<double, double>(h);
+            const double* in = h->r1.p;
+            double* outp = h->r2.p;
+            void* args[] = {&a, (void*)&in, (void*)&outp};
+            launch_coop(h, (const void*)k_apply<double, double>, args);
         }
         copy_out(h, z, h->r2.p, h->m);
     });
@@ -1106,10 +1104,10 @@ int psipm_matvec(psipm_handle* h, const double* v, double* y) {
     if (!v || !y) return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
         require(h->have_theta, PSIPM_ERR_STATE, "matvec before set_theta");
-        PcgArgs<double> a = pcg_args<double>(h);  // the operator is always applied in FP64 here
+        PcgArgs<double, double> a = pcg_args<double, double>(h);  // the operator is applied in FP64 here
         PSIPM_CUDA(cudaMemcpyAsync(h->p64.p.p, v, h->m * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         void* args[] = {&a};
-        launch_coop(h, (const void*)k_matvec<double>, args);
+        launch_coop(h, (const void*)k_matvec<double, double>, args);
         copy_out(h, y, h->p64.q.p, h->m);
     });
 }
@@ -1204,6 +1202,11 @@ __global__ void k_scale_narrow(long long m, const double* __restrict__ r, double
     if (i < m) out[i] = (float)(r[i] * s);
 }
 
+__global__ void k_axpy64(long long m, const double* __restrict__ d, double* __restrict__ x) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < m) x[i] += d[i];
+}
+
 __global__ void k_axpy_widen(long long m, double a, const float* __restrict__ d, double* __restrict__ x) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < m) x[i] += a * (double)d[i];
@@ -1238,7 +1241,10 @@ const double* solve_normal(psipm_handle* h, const double* rhs, double tol, int m
                            double gap_tol, psipm_pcg_info* info) {
     require(h->have_factor, PSIPM_ERR_STATE, "solve before a successful factor");
     if (h->precision != PSIPM_FP32_REFINED) {
-        run_pcg<double>(h, rhs, tol, maxit, variant, replacement, gap_tol, info);
+        if (h->precision == PSIPM_FP32_PRECOND)
+            run_pcg<double, float>(h, rhs, tol, maxit, variant, replacement, gap_tol, info);
+        else
+            run_pcg<double, double>(h, rhs, tol, maxit, variant, replacement, gap_tol, info);
         h->r64.reserve(h->m);
         PSIPM_CUDA(cudaMemcpyAsync(h->r64.p, h->p64.tr.p, h->m * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         return h->p64.x.p;
@@ -1247,7 +1253,7 @@ const double* solve_normal(psipm_handle* h, const double* rhs, double tol, int m
     cudaStream_t st = h->stream;
     h->x64.zero(m, st);
     PcgStore<float>& s32 = h->p32;
-    pcg_args<float>(h);  // sizes the FP32 work vectors
+    pcg_args<float, float>(h);  // sizes the FP32 work vectors
     double rnorm = fp64_residual(h, rhs, h->x64.p);
     const double rhs_norm = rnorm;
     const double scale = variant == PSIPM_PCG_HSD ? rhs_norm : std::max(1.0, rhs_norm);
@@ -1265,7 +1271,7 @@ const double* solve_normal(psipm_handle* h, const double* rhs, double tol, int m
         LAUNCH(h, k_scale_narrow<<<blocks_for(m, 256), 256, 0, st>>>(m, h->r64.p, 1.0 / rnorm, s32.rhs.p));
         const double inner = std::min(0.5, std::max(1e-5, 0.5 * target / rnorm));
         psipm_pcg_info one;
-        run_pcg<float>(h, s32.rhs.p, inner, budget, variant, replacement, gap_tol, &one);
+        run_pcg<float, float>(h, s32.rhs.p, inner, budget, variant, replacement, gap_tol, &one);
         if (sweeps == 0) first = one;
         last_info = one.info;
         total.iterations += one.iterations;
@@ -1276,10 +1282,30 @@ const double* solve_normal(psipm_handle* h, const double* rhs, double tol, int m
         for (int q = 0; q < 4; ++q) total.phase_seconds[q] += one.phase_seconds[q];
         budget -= std::max(1, one.iterations);
         LAUNCH(h, k_axpy_widen<<<blocks_for(m, 256), 256, 0, st>>>(m, rnorm, s32.x.p, h->x64.p));
+        const double before = rnorm;
         rnorm = fp64_residual(h, rhs, h->x64.p);
         ++sweeps;
-        if (one.iterations == 0 && one.info != 0) break;  // no progress possible
         if (!std::isfinite(rnorm)) break;
+        if (rnorm > 0.1 * before && rnorm > target) {
+            // FP32 arithmetic cannot reduce this residual further (the
+            // operator's rounding error is comparable to it): finish with an
+            // FP64 PCG around the FP32 preconditioner, from the current x.
+            psipm_pcg_info tail;
+            pcg_args<double, double>(h);  // sizes the FP64 work vectors
+            PSIPM_CUDA(cudaMemcpyAsync(h->p64.rhs.p, h->r64.p, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            const double tail_tol = std::max(1e-16, std::min(0.5, target / std::max(rnorm, 1e-300)));
+            run_pcg<double, float>(h, h->p64.rhs.p, tail_tol, std::max(1, budget), PSIPM_PCG_HSD, replacement,
+                                   gap_tol, &tail);
+            total.iterations += tail.iterations;
+            total.matvecs += tail.matvecs;
+            total.seconds += tail.seconds;
+            for (int q = 0; q < 4; ++q) total.phase_seconds[q] += tail.phase_seconds[q];
+            LAUNCH(h, k_axpy64<<<blocks_for(m, 256), 256, 0, st>>>(m, h->p64.x.p, h->x64.p));
+            rnorm = fp64_residual(h, rhs, h->x64.p);
+            ++sweeps;
+            last_info = tail.ok ? 0 : tail.info;
+            break;
+        }
     }
     if (info) {
         *info = total;
@@ -1356,7 +1382,7 @@ int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t
     return guarded(h, [&]() {
         require(h->have_factor, PSIPM_ERR_STATE, "apply before a successful factor");
         require(h->precision == PSIPM_FP64, PSIPM_ERR_UNSUPPORTED, "apply trace is FP64 only");
-        PcgArgs<double> a = pcg_args<double>(h);
+        PcgArgs<double, double> a = pcg_args<double, double>(h);
         DevBuf<long long> tr;
         tr.zero(cap, h->stream);
         a.pc.trace = tr.p;
@@ -1366,7 +1392,7 @@ int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t
         const double* in = h->r1.p;
         double* outp = h->r2.p;
         void* args[] = {&a, (void*)&in, (void*)&outp};
-        launch_coop(h, (const void*)k_apply<double>, args);
+        launch_coop(h, (const void*)k_apply<double, double>, args);
         copy_out(h, z, h->r2.p, h->m);
         std::vector<long long> host(cap);
         PSIPM_CUDA(cudaMemcpyAsync(host.data(), tr.p, cap * sizeof(long long), cudaMemcpyDeviceToHost, h->stream));

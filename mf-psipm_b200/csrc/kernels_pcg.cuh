@@ -83,14 +83,14 @@ struct PrecLayout {
     T* uvec = nullptr;
 };
 
-template <typename T>
+template <typename T, typename P = T>
 struct PcgArgs {
     SpmvLayout sp;
     const T* at_val = nullptr;
     const T* a_val = nullptr;
     const T* w = nullptr;
     T delta = 0;
-    PrecLayout<T> pc;
+    PrecLayout<P> pc;
     const T* rhs = nullptr;
     T* x = nullptr;
     T* r = nullptr;
@@ -146,8 +146,8 @@ __device__ __forceinline__ void read_totals(const double* part, double (&tot)[K]
 
 // ---- phase A: t = w o (A^T src) -----------------------------------------
 // src: 0 -> v, 1 -> z, 2 -> z + beta p
-template <typename T>
-__device__ void phase_a(const PcgArgs<T>& a, const T* v, int src, T beta) {
+template <typename T, typename P>
+__device__ void phase_a(const PcgArgs<T, P>& a, const T* v, int src, T beta) {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
     const int* __restrict__ ptr = a.sp.at_ptr;
@@ -174,8 +174,8 @@ __device__ void phase_a(const PcgArgs<T>& a, const T* v, int src, T beta) {
 // mode 0: p = src(p'); q = At + delta p; acc += {p.q, p.p, q.q}
 // mode 1: tr = rhs - (At + delta x); acc += {tr.tr, (tr-r).(tr-r)}
 // mode 2: r = rhs - (At + delta x); acc += {r.r}
-template <typename T>
-__device__ __forceinline__ void row_epilogue(const PcgArgs<T>& a, int mode, int src, T beta, int i,
+template <typename T, typename P>
+__device__ __forceinline__ void row_epilogue(const PcgArgs<T, P>& a, int mode, int src, T beta, int i,
                                              T s, double (&acc)[3]) {
     if (mode == 0) {
         T pn = src == 1 ? a.z[i] : (src == 2 ? a.z[i] + beta * a.p[i] : a.p[i]);
@@ -198,8 +198,8 @@ __device__ __forceinline__ void row_epilogue(const PcgArgs<T>& a, int mode, int 
     }
 }
 
-template <typename T>
-__device__ void phase_b(const PcgArgs<T>& a, int mode, int src, T beta, double (&acc)[3]) {
+template <typename T, typename P>
+__device__ void phase_b(const PcgArgs<T, P>& a, int mode, int src, T beta, double (&acc)[3]) {
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -231,8 +231,8 @@ __device__ void phase_b(const PcgArgs<T>& a, int mode, int src, T beta, double (
     }
 }
 
-template <typename T>
-__device__ void phase_b2(const PcgArgs<T>& a, int mode, int src, T beta, double (&acc)[3]) {
+template <typename T, typename P>
+__device__ void phase_b2(const PcgArgs<T, P>& a, int mode, int src, T beta, double (&acc)[3]) {
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
     for (int l = gtid; l < a.sp.n_long; l += gstride) {
@@ -281,19 +281,18 @@ __device__ __forceinline__ void warp_dot4(const T* __restrict__ m0, const T* __r
 }
 
 // forward pre-phase: f into fvec, outputs initialised (x_s = 0, u_s = f_bot)
-template <typename T>
-__device__ void prec_forward_pre(const PcgArgs<T>& a, const T* in, int4 task) {
-    const PrecLayout<T>& pc = a.pc;
+template <typename P, typename IT>
+__device__ void prec_forward_pre(const PrecLayout<P>& pc, const IT* in, int4 task) {
     const int lane = threadIdx.x & 31;
     const int s = task.x;
     const int first = pc.sn_first[s];
     const int c = pc.sn_first[s + 1] - first;
     const long long rb = pc.sn_rowptr[s];
     for (int q = task.y + lane; q < task.z; q += 32) {
-        T f = 0;
+        P f = 0;
         if (q < c) {
             const int k = first + q;
-            f = pc.dscp[k] * in[pc.perm[k]];
+            f = pc.dscp[k] * (P)in[pc.perm[k]];
         }
         for (long long g = pc.fg_ptr[rb + q]; g < pc.fg_ptr[rb + q + 1]; ++g) f += pc.uvec[pc.fg_idx[g]];
         pc.fvec[rb + q] = f;
@@ -305,19 +304,18 @@ __device__ void prec_forward_pre(const PcgArgs<T>& a, const T* in, int4 task) {
 }
 
 // forward task {s, i0, i1, j0}: rows [i0, i1) of G against f[j0, j0+chunk)
-template <typename T>
-__device__ void prec_forward_gemv(const PcgArgs<T>& a, int4 task) {
-    const PrecLayout<T>& pc = a.pc;
+template <typename P>
+__device__ void prec_forward_gemv(const PrecLayout<P>& pc, int4 task) {
     const int lane = threadIdx.x & 31;
     const int s = task.x, i0 = task.y, i1 = task.z, j0 = task.w;
     const int first = pc.sn_first[s];
     const int c = pc.sn_first[s + 1] - first;
     const int j1 = min(c, j0 + kApplyChunk);
     const long long rb = pc.sn_rowptr[s];
-    const T* __restrict__ Gs = pc.G + pc.panel_off[s];
-    const T* __restrict__ f = pc.fvec + rb;
+    const P* __restrict__ Gs = pc.G + pc.panel_off[s];
+    const P* __restrict__ f = pc.fvec + rb;
     for (int i = i0; i < i1; i += 4) {
-        const T* rows[4];
+        const P* rows[4];
         int end[4];
         for (int k = 0; k < 4; ++k) {
             const int ii = min(i + k, i1 - 1);
@@ -325,11 +323,11 @@ __device__ void prec_forward_gemv(const PcgArgs<T>& a, int4 task) {
             end[k] = i + k < i1 ? (ii < c ? min(j1, ii + 1) : j1) : j0;  // G_top is lower triangular
         }
         // rows share the loop bound j1; entries past a row's own end are masked
-        T d[4];
+        P d[4];
         const int lo = j0;
-        T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        P s0 = 0, s1 = 0, s2 = 0, s3 = 0;
         for (int j = lo + lane; j < j1; j += 32) {
-            const T fj = f[j];
+            const P fj = f[j];
             if (j < end[0]) s0 += rows[0][j] * fj;
             if (j < end[1]) s1 += rows[1][j] * fj;
             if (j < end[2]) s2 += rows[2][j] * fj;
@@ -341,7 +339,7 @@ __device__ void prec_forward_gemv(const PcgArgs<T>& a, int4 task) {
         d[3] = warp_sum(s3);
         if (lane < 4 && i + lane < i1) {
             const int ii = i + lane;
-            const T v = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
+            const P v = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
             if (ii < c)
                 atomicAdd(&pc.xp[first + ii], v);
             else
@@ -351,9 +349,8 @@ __device__ void prec_forward_gemv(const PcgArgs<T>& a, int4 task) {
 }
 
 // backward pre-phase: v into bvec, y_s = 0
-template <typename T>
-__device__ void prec_backward_pre(const PcgArgs<T>& a, int4 task) {
-    const PrecLayout<T>& pc = a.pc;
+template <typename P>
+__device__ void prec_backward_pre(const PrecLayout<P>& pc, int4 task) {
     const int lane = threadIdx.x & 31;
     const int s = task.x;
     const int first = pc.sn_first[s];
@@ -366,29 +363,28 @@ __device__ void prec_backward_pre(const PcgArgs<T>& a, int4 task) {
 }
 
 // backward task {s, j0, j1, i0}: columns [j0, j1) of G (rows of GT) against v[i0, i0+chunk)
-template <typename T>
-__device__ void prec_backward_gemv(const PcgArgs<T>& a, int4 task) {
-    const PrecLayout<T>& pc = a.pc;
+template <typename P>
+__device__ void prec_backward_gemv(const PrecLayout<P>& pc, int4 task) {
     const int lane = threadIdx.x & 31;
     const int s = task.x, j0 = task.y, j1 = task.z, i0 = task.w;
     const int first = pc.sn_first[s];
     const long long rb = pc.sn_rowptr[s];
     const int r = (int)(pc.sn_rowptr[s + 1] - rb);
     const int i1 = min(r, i0 + kApplyChunk);
-    const T* __restrict__ GTs = pc.GT + pc.gt_off[s];
-    const T* __restrict__ v = pc.bvec + rb;
+    const P* __restrict__ GTs = pc.GT + pc.gt_off[s];
+    const P* __restrict__ v = pc.bvec + rb;
     for (int j = j0; j < j1; j += 4) {
-        const T* rows[4];
+        const P* rows[4];
         int beg[4];
         for (int k = 0; k < 4; ++k) {
             const int jj = min(j + k, j1 - 1);
             rows[k] = GTs + (long long)jj * r;
             beg[k] = j + k < j1 ? max(i0, jj) : i1;  // G[i, j] = 0 for i < j
         }
-        T d[4];
+        P d[4];
         warp_dot4(rows[0], rows[1], rows[2], rows[3], v, beg[0], beg[1], beg[2], beg[3], i1, d);
         if (lane < 4 && j + lane < j1) {
-            const T val = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
+            const P val = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
             atomicAdd(&pc.yp[first + j + lane], val);
         }
     }
@@ -399,29 +395,28 @@ __device__ void prec_backward_gemv(const PcgArgs<T>& a, int4 task) {
 // output, so no pre-phase, no shuffles and no atomics are needed.
 constexpr int kSmallRows = 64;
 
-template <typename T>
-__device__ void prec_forward_small(const PcgArgs<T>& a, const T* in, int s, T* fs) {
-    const PrecLayout<T>& pc = a.pc;
+template <typename P, typename IT>
+__device__ void prec_forward_small(const PrecLayout<P>& pc, const IT* in, int s, P* fs) {
     const int lane = threadIdx.x & 31;
     const int first = pc.sn_first[s];
     const int c = pc.sn_first[s + 1] - first;
     const long long rb = pc.sn_rowptr[s];
     const int r = (int)(pc.sn_rowptr[s + 1] - rb);
     for (int q = lane; q < r; q += 32) {
-        T f = 0;
+        P f = 0;
         if (q < c) {
             const int k = first + q;
-            f = pc.dscp[k] * in[pc.perm[k]];
+            f = pc.dscp[k] * (P)in[pc.perm[k]];
         }
         for (long long g = pc.fg_ptr[rb + q]; g < pc.fg_ptr[rb + q + 1]; ++g) f += pc.uvec[pc.fg_idx[g]];
         fs[q] = f;
     }
     __syncwarp();
-    const T* __restrict__ Gs = pc.G + pc.panel_off[s];
+    const P* __restrict__ Gs = pc.G + pc.panel_off[s];
     for (int row = lane; row < r; row += 32) {
         const int jlim = row < c ? row + 1 : c;
-        const T* __restrict__ g = Gs + (long long)row * c;
-        T d = 0;
+        const P* __restrict__ g = Gs + (long long)row * c;
+        P d = 0;
         for (int j = 0; j < jlim; ++j) d += g[j] * fs[j];
         if (row < c)
             pc.xp[first + row] = d;
@@ -431,9 +426,8 @@ __device__ void prec_forward_small(const PcgArgs<T>& a, const T* in, int s, T* f
     __syncwarp();
 }
 
-template <typename T>
-__device__ void prec_backward_small(const PcgArgs<T>& a, int s, T* fs) {
-    const PrecLayout<T>& pc = a.pc;
+template <typename P>
+__device__ void prec_backward_small(const PrecLayout<P>& pc, int s, P* fs) {
     const int lane = threadIdx.x & 31;
     const int first = pc.sn_first[s];
     const int c = pc.sn_first[s + 1] - first;
@@ -442,8 +436,8 @@ __device__ void prec_backward_small(const PcgArgs<T>& a, int s, T* fs) {
     for (int q = lane; q < r; q += 32) fs[q] = q < c ? pc.xp[first + q] : -pc.yp[pc.sn_rows[rb + q]];
     __syncwarp();
     if (lane < c) {
-        const T* __restrict__ gt = pc.GT + pc.panel_off[s] + (long long)lane * r;
-        T d = 0;
+        const P* __restrict__ gt = pc.GT + pc.panel_off[s] + (long long)lane * r;
+        P d = 0;
         for (int i = lane; i < r; ++i) d += gt[i] * fs[i];
         pc.yp[first + lane] = d;
     }
@@ -452,10 +446,9 @@ __device__ void prec_backward_small(const PcgArgs<T>& a, int s, T* fs) {
 
 // z = P^{-1} in; acc_rz += in . z.  Ends without a barrier (the caller's
 // reduction provides it).
-template <typename T>
-__device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc_rz, T* fs,
+template <typename P, typename IT>
+__device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, double& acc_rz, P* fs,
                            cgx::grid_group& grid) {
-        const PrecLayout<T>& pc = a.pc;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     int ntrace = 0;
@@ -468,16 +461,16 @@ __device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc
     for (int lev = 0; lev < pc.nlevels; ++lev) {
         if (pc.fpre_ptr[lev + 1] > pc.fpre_ptr[lev]) {
             for (int tk = pc.fpre_ptr[lev] + gwarp; tk < pc.fpre_ptr[lev + 1]; tk += nwarps)
-                prec_forward_pre(a, in, pc.fpre_tasks[tk]);
+                prec_forward_pre(pc, in, pc.fpre_tasks[tk]);
             grid.sync();
             mark();
         }
         for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps) {
             const int4 task = pc.fwd_tasks[tk];
             if (task.w < 0)
-                prec_forward_small(a, in, task.x, fs);
+                prec_forward_small(pc, in, task.x, fs);
             else
-                prec_forward_gemv(a, task);
+                prec_forward_gemv(pc, task);
         }
         grid.sync();
         mark();
@@ -485,16 +478,16 @@ __device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc
     for (int lev = pc.nlevels - 1; lev >= 0; --lev) {
         if (pc.bpre_ptr[lev + 1] > pc.bpre_ptr[lev]) {
             for (int tk = pc.bpre_ptr[lev] + gwarp; tk < pc.bpre_ptr[lev + 1]; tk += nwarps)
-                prec_backward_pre(a, pc.bpre_tasks[tk]);
+                prec_backward_pre(pc, pc.bpre_tasks[tk]);
             grid.sync();
             mark();
         }
         for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps) {
             const int4 task = pc.bwd_tasks[tk];
             if (task.w < 0)
-                prec_backward_small(a, task.x, fs);
+                prec_backward_small(pc, task.x, fs);
             else
-                prec_backward_gemv(a, task);
+                prec_backward_gemv(pc, task);
         }
         grid.sync();
         mark();
@@ -503,7 +496,7 @@ __device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc
     const int gstride = gridDim.x * blockDim.x;
     for (int i = gtid; i < pc.m; i += gstride) {
         const int k = pc.iperm[i];
-        const T zi = pc.dscp[k] * pc.yp[k];
+        const IT zi = (IT)(pc.dscp[k] * pc.yp[k]);
         out[i] = zi;
         acc_rz += (double)in[i] * (double)zi;
     }
@@ -511,8 +504,8 @@ __device__ void prec_apply(const PcgArgs<T>& a, const T* in, T* out, double& acc
 
 // H v into phase-B epilogue `mode` (A, barrier, B [, barrier, B2]); ends after
 // the partials are written; the caller issues the barrier.
-template <typename T>
-__device__ void operator_pass(const PcgArgs<T>& a, const T* v, int src, T beta, int mode,
+template <typename T, typename P>
+__device__ void operator_pass(const PcgArgs<T, P>& a, const T* v, int src, T beta, int mode,
                               double (&acc)[3], cgx::grid_group& grid) {
     phase_a(a, v, src, beta);
     grid.sync();
@@ -523,12 +516,12 @@ __device__ void operator_pass(const PcgArgs<T>& a, const T* v, int src, T beta, 
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T> a) {
+template <typename T, typename P>
+__global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T, P> a) {
     cgx::grid_group grid = cgx::this_grid();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double scratch[kPcgWarps + 1];
-    T* fs = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
+    P* fs = reinterpret_cast<P*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
     const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
@@ -552,29 +545,29 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T> a) {
         }
     };
     auto reduce1 = [&](double v) -> double {
-        double* P = a.part + (size_t)(red & 1) * gridDim.x * 4;
+        double* pb = a.part + (size_t)(red & 1) * gridDim.x * 4;
         double acc[1] = {v}, tot[1];
-        write_partials<1>(acc, P, scratch);
+        write_partials<1>(acc, pb, scratch);
         grid.sync();
-        read_totals<1>(P, tot, scratch);
+        read_totals<1>(pb, tot, scratch);
         ++red;
         return tot[0];
     };
     auto reduce2 = [&](double (&acc)[3], double (&tot)[3]) {
-        double* P = a.part + (size_t)(red & 1) * gridDim.x * 4;
+        double* pb = a.part + (size_t)(red & 1) * gridDim.x * 4;
         double a2[2] = {acc[0], acc[1]}, t2[2];
-        write_partials<2>(a2, P, scratch);
+        write_partials<2>(a2, pb, scratch);
         grid.sync();
-        read_totals<2>(P, t2, scratch);
+        read_totals<2>(pb, t2, scratch);
         tot[0] = t2[0];
         tot[1] = t2[1];
         ++red;
     };
     auto reduce3 = [&](double (&acc)[3], double (&tot)[3]) {
-        double* P = a.part + (size_t)(red & 1) * gridDim.x * 4;
-        write_partials<3>(acc, P, scratch);
+        double* pb = a.part + (size_t)(red & 1) * gridDim.x * 4;
+        write_partials<3>(acc, pb, scratch);
         grid.sync();
-        read_totals<3>(P, tot, scratch);
+        read_totals<3>(pb, tot, scratch);
         ++red;
     };
 
@@ -596,7 +589,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T> a) {
     {
         // x = P^-1 rhs ; r = rhs - H x
         double dummy = 0.0;
-        prec_apply(a, a.rhs, a.x, dummy, fs, grid);
+        prec_apply(a.pc, a.rhs, a.x, dummy, fs, grid);
         grid.sync();
         acc3[0] = acc3[1] = acc3[2] = 0.0;
         operator_pass(a, a.x, 0, (T)0, 2, acc3, grid);
@@ -613,7 +606,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T> a) {
             nhist = 1;
         }
         double rzacc = 0.0;
-        prec_apply(a, a.r, a.z, rzacc, fs, grid);
+        prec_apply(a.pc, a.r, a.z, rzacc, fs, grid);
         rz = reduce1(rzacc);
         if (hsd) {
             if (!finite_d(rz) || rz <= 0.0) goto done;
@@ -717,7 +710,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T> a) {
                     ++repl;
                     grid.sync();
                     double rzr = 0.0;
-                    prec_apply(a, a.r, a.z, rzr, fs, grid);
+                    prec_apply(a.pc, a.r, a.z, rzr, fs, grid);
                     rz = reduce1(rzr);
                     if (!finite_d(rz) || rz <= 0.0) {
                         info = -5;
@@ -733,7 +726,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T> a) {
         // z = P^-1 r ; beta
         lap(3);
         double rzn = 0.0;
-        prec_apply(a, a.r, a.z, rzn, fs, grid);
+        prec_apply(a.pc, a.r, a.z, rzn, fs, grid);
         const double rz_next = reduce1(rzn);
         lap(2);
         if (!finite_d(rz_next) || rz_next <= 0.0) {
@@ -790,18 +783,18 @@ __global__ void k_barrier_probe(int count, long long* out) {
 }
 
 // Standalone preconditioner apply / operator kernels (cooperative as well)
-template <typename T>
-__global__ void __launch_bounds__(kPcgThreads, 3) k_apply(PcgArgs<T> a, const T* in, T* out) {
+template <typename T, typename P>
+__global__ void __launch_bounds__(kPcgThreads, 3) k_apply(PcgArgs<T, P> a, const T* in, T* out) {
     cgx::grid_group grid = cgx::this_grid();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* fs = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
+    P* fs = reinterpret_cast<P*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
     double dummy = 0.0;
-    prec_apply(a, in, out, dummy, fs, grid);
+    prec_apply(a.pc, in, out, dummy, fs, grid);
 }
 
 // y = H v  (mode 0 with src = v copied into p first by the host)
-template <typename T>
-__global__ void __launch_bounds__(kPcgThreads, 3) k_matvec(PcgArgs<T> a) {
+template <typename T, typename P>
+__global__ void __launch_bounds__(kPcgThreads, 3) k_matvec(PcgArgs<T, P> a) {
     cgx::grid_group grid = cgx::this_grid();
     double acc[3] = {0.0, 0.0, 0.0};
     operator_pass(a, a.p, 0, (T)0, 0, acc, grid);

@@ -34,6 +34,7 @@ PCG_SPECTRAL = 0
 PCG_HSD = 1
 FP64 = 0
 FP32_REFINED = 1
+FP32_PRECOND = 2
 
 STATUS_NAMES = {
     ERR_ARGUMENT: "invalid argument",

@@ -517,7 +517,7 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self.pcg_matvecs += res.matvecs
         self.pcg_replacements += res.replacements
         self.pcg_phase_seconds += np.asarray(res.phase_seconds)
-        bv = 4 if self.precision == _lib.FP32_REFINED else 8
+        bv = 4 if self.precision != _lib.FP64 else 8
         self.pcg_bytes += pcg_launch_bytes(self.m, self.n, self.A.nnz, self.nnz_factor, res.iterations,
                                            res.matvecs, res.iterations + 2 + res.replacements, bv)
         self.refinement_sweeps += res.refinements

@@ -1,4 +1,5 @@
-"""FP32 factor / PCG with FP64 refinement against the exact direction.
+"""FP32 modes against the exact direction: FP32 factor / PCG with FP64
+refinement (mode 1) and FP64 PCG around an FP32 preconditioner (mode 2).
 
 Bars: with tolerance 1e-10 the refined direction is within 1e-8 of the
 exact one (the same bar as FP64 mode at 1e-13 would give 1e-8); the FP32
@@ -14,18 +15,22 @@ from _helpers import NAMES, OPTIONS, exact_direction, lp_from, rel
 pytestmark = pytest.mark.gpu
 
 
-def devices(lp):
+MODES = (1, 2)  # FP32_REFINED, FP32_PRECOND
+
+
+def devices(lp, mode):
     from psipm_b200 import _lib
     from psipm_b200.device import NormalEquationsDevice
 
-    return NormalEquationsDevice(lp.A, precision=_lib.FP64), NormalEquationsDevice(lp.A, precision=_lib.FP32_REFINED)
+    return NormalEquationsDevice(lp.A, precision=_lib.FP64), NormalEquationsDevice(lp.A, precision=mode)
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", NAMES)
-def test_fp32_refined_directions(name, golden):
+def test_fp32_refined_directions(name, mode, golden):
     g = golden(name)
     lp = lp_from(g)
-    d64, d32 = devices(lp)
+    d64, d32 = devices(lp, mode)
     for i in range(min(6, int(g["n_solve_calls"]))):
         theta, delta = g[f"s{i}_theta"], float(g[f"s{i}_delta"])
         for d in (d64, d32):
@@ -39,19 +44,20 @@ def test_fp32_refined_directions(name, golden):
         assert res.info == 0 and res.relative_residual <= 1e-10, (i, res.info, res.relative_residual)
         assert rel(res.x, dy_e) <= 1e-8, i
         assert rel(dx, dx_e) <= 1e-8, i
-        assert res.refinements >= 1
+        if mode == 1:
+            assert res.refinements >= 1
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", NAMES)
-def test_fp32_refined_full_solve(name, golden):
+def test_fp32_refined_full_solve(name, mode, golden):
     from oracle import ipm as OI
     from psipm_b200 import _lib
     from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner
 
     g = golden(name)
     lp = lp_from(g)
-    solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, precision=_lib.FP32_REFINED,
-                                                   **OPTIONS)
+    solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, precision=mode, **OPTIONS)
     sol = OI.psipm_solve(lp, solver, tol=1e-8)
     assert sol.status == "optimal"
     ref = float(g["obj"])
