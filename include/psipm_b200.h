@@ -170,6 +170,80 @@ int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev,
                     int32_t maxit, int32_t variant, int32_t replacement, double gap_tolerance,
                     double* dx_dev, double* dy_dev, psipm_pcg_info* info);
 
+/* ---- device-resident PS-IPM inner loop ------------------------------------------
+ * The reference's prox_eval (psipm_active_pool.py:1947-2271) and the outer
+ * KKT measures of psipm_solve (:2559-2637) do their O(n) arithmetic in NumPy
+ * and pass theta, r1, r2 across the KKT boundary and dx, dy back.  These
+ * entry points keep the whole iterate in device memory instead: the handle
+ * holds the LP data (c, b, u, pos, box), the iterate (x, y, z, w, s), the
+ * proximal centre (xk, yk, zk, wk), the residuals (rd, rp), the
+ * complementarity targets (rmz, rmw), a direction D = (dx, dy, dz, dw) and a
+ * corrector C = (dxc, dyc, dzc, dwc).  The host keeps only the scalars the
+ * loop branches on.  Sums are reproducible to rounding (block partials are
+ * combined in no fixed order); minima and maxima are exact.  */
+
+/* Upload c[n], b[m], u[n] and the masks pos[n], box[n] (0/1 bytes) and
+ * allocate the vectors (psipm_active_pool.py:2389-2392). */
+int psipm_ipm_load(psipm_handle* h, const double* c, const double* b, const double* u,
+                   const uint8_t* pos, const uint8_t* box);
+/* Host <-> device copies of one vector set (x[n], y[m], z[n], w[n]):
+ * which = 0 the iterate (x, y, z, w), 1 the centre (xk, yk, zk, wk),
+ * 2 the direction D (dx, dy, dz, dw), 3 the corrector C (dxc, dyc, dzc, dwc). */
+int psipm_ipm_put(psipm_handle* h, int32_t which, const double* x, const double* y,
+                  const double* z, const double* w);
+int psipm_ipm_get(psipm_handle* h, int32_t which, double* x, double* y, double* z, double* w);
+/* to_centre = 1: centre <- iterate (psipm_active_pool.py:2670-2672).  to_centre = 0:
+ * iterate <- centre, s = 1, then the box floors x = clip(x, x_floor, u - s_floor),
+ * s = max(u - x, s_floor) on box columns (:1963-1967, sync_box :1860-1872). */
+int psipm_ipm_copy(psipm_handle* h, int32_t to_centre);
+/* Proximal residuals of the iterate (:1984-1993): rd = -(c - A^T y - z + w + rho (x - xk)),
+ * rp = -(A x - b + delta (y - yk)) stay on the device; out[6] =
+ * {sum_pos x z + sum_box s w, |gp|^2, |rp|^2, |rd|^2, |x - xk|^2, |y - yk|^2} with
+ * g = c - A^T y + rho (x - xk) and gp = x - clip(x - g, 0, u) on pos, g elsewhere. */
+int psipm_ipm_residuals(psipm_handle* h, double rho, double delta, double* out);
+/* theta = theta_min + pos z/x + box w/s, non-finite entries -> theta_cap, clipped to
+ * [theta_min, theta_cap] (:2014-2020), written as the handle's theta; then the
+ * same as psipm_set_theta(h, theta, delta) without the host copy. */
+int psipm_ipm_theta(psipm_handle* h, double theta_min, double theta_cap, double delta);
+/* Complementarity targets rmz (pos), rmw (box):
+ *   kind 0: -x z + p[0], -s w + p[0]                     (:2063-2087)
+ *   kind 1: p[0] - dx dz, p[0] - ds dw, ds = -dx          (Mehrotra, :2113-2114)
+ *   kind 2: Gondzio, p = {ta_x, ta_z, mu_target, beta_min, beta_max}:
+ *           prod = (x + ta_x dx)(z + ta_z dz) (and (s - ta_x dx)(w + ta_z dw)),
+ *           clip(clip(prod, bmin mu, bmax mu) - prod, -bmax mu, 2 bmax mu)  (:2180-2197) */
+int psipm_ipm_targets(psipm_handle* h, int32_t kind, const double* params);
+/* One Newton system (newton(), :2042-2056): r1 = rd + rmz/x - rmw/s, r2 = rp
+ * into D (corrector = 0), or r1 = rmz/x - rmw/s, r2 = 0 into C (corrector = 1);
+ * (dx, dy) = psipm_solve_dev(r1, r2, ...), dz = (rmz - z dx)/x on pos,
+ * dw = (rmw + w dx)/s on box.  *finite = 0 when dx, dy, dz or dw holds a
+ * non-finite entry.  alphas/betas/history (may be NULL) and info as in
+ * psipm_solve. */
+int psipm_ipm_newton(psipm_handle* h, int32_t corrector, double tol, int32_t maxit,
+                     int32_t variant, int32_t replacement, double gap_tolerance, double* alphas,
+                     double* betas, double* history, int32_t* finite, psipm_pcg_info* info);
+/* Step to the boundary (_step_to_boundary, :1831-1837) along d = D (with_corrector
+ * = 0) or d = D + gamma C: out[0] = min(1, min_{pos,dx<0} -x/dx, min_{box,ds<0} -s/ds),
+ * out[1] = min(1, min_{pos,dz<0} -z/dz, min_{box,dw<0} -w/dw); ds = -dx. */
+int psipm_ipm_steps(psipm_handle* h, int32_t with_corrector, double gamma, double* out);
+/* *out = sum_pos (x + ax dx)(z + az dz) + sum_box (s - ax dx)(w + az dw) along
+ * d = D or D + gamma C (trial mu, :2109-2110 and :2124-2128). */
+int psipm_ipm_complementarity(psipm_handle* h, int32_t with_corrector, double gamma,
+                              double alpha_x, double alpha_z, double* out);
+/* D += gamma C (the accepted corrector, :2142-2145 and :2200-2203). */
+int psipm_ipm_accept(psipm_handle* h, double gamma);
+/* x += ax dx, y += az dy, z += az dz, w += az dw, then the box floors (:2231-2236). */
+int psipm_ipm_update(psipm_handle* h, double alpha_x, double alpha_z);
+/* Outer KKT measures (:2561-2599) after the box floors on the iterate:
+ * out[6] = {max|b - A x|, max|c - A^T y - z + w|, c.x, b.y, sum_box w u,
+ * sum_pos x z + sum_box s w}. */
+int psipm_ipm_metrics(psipm_handle* h, double* out);
+/* Lag bound of the spectral rule (psipm_spectral_preconditioner.py:396-410):
+ * psipm_lag_reference keeps the current weights w = 1/theta as the reference;
+ * psipm_lag_ratio returns out = {max r, min r} over r = w / max(w_ref, tiny),
+ * or {inf, 0} if some r is not finite and positive. */
+int psipm_lag_reference(psipm_handle* h);
+int psipm_lag_ratio(psipm_handle* h, double* out);
+
 /* ---- diagnostics ---------------------------------------------------------------- */
 /* Device-side stopwatch on the handle's stream (CUDA events): start records
  * an event; stop records a second one, waits for it and returns the elapsed

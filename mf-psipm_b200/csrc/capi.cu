@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "kernels_factor.cuh"
+#include "kernels_ipm.cuh"
 #include "kernels_pcg.cuh"
 #include "kernels_select.cuh"
 #include "symbolic.h"
@@ -48,6 +49,22 @@ struct FactorStore {
 template <typename T>
 struct PcgStore {
     DevBuf<T> rhs, x, r, z, p, q, t, tr, chunk_part, w, at_val, a_val;
+};
+
+// Device-resident PS-IPM state: LP data, iterate (x, y, z, w, s), proximal
+// centre (xk, yk, zk, wk), residuals, complementarity targets, the Newton
+// direction D = (dx, dy, dz, dw) and the corrector C = (dxc, dyc, dzc, dwc).
+struct IpmStore {
+    bool loaded = false;
+    DevBuf<double> c, b, u;
+    DevBuf<unsigned char> pos, box;
+    DevBuf<double> x, y, z, w, s, xk, yk, zk, wk;
+    DevBuf<double> rd, rp, rmz, rmw, r1, zero_m, aty, ax;
+    DevBuf<double> dx, dy, dz, dw, dxc, dyc, dzc, dwc;
+    DevBuf<double> red, wref;
+    DevBuf<unsigned long long> redu;
+    DevBuf<int> flag;
+    bool have_ref = false;
 };
 
 }  // namespace
@@ -129,6 +146,9 @@ struct psipm_handle {
     DevBuf<int> ctrl, iout;
     DevBuf<double> dout, alphas, betas, history;
     DevBuf<double> r1, r2, dx, dy, wr1;
+
+    // PS-IPM vectors
+    IpmStore ipm;
 
     // selection scratch
     DevBuf<unsigned char> flag_a, flag_b, flag_c, mand_flags;
@@ -1435,6 +1455,350 @@ int psipm_timer_stop(psipm_handle* h, double* seconds) {
 int psipm_set_profiling(psipm_handle* h, int32_t on) {
     (void)on;
     return h ? PSIPM_OK : PSIPM_ERR_ARGUMENT;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Device-resident PS-IPM vectors (kernels_ipm.cuh).  The inner loop of the
+// reference's prox_eval (psipm_active_pool.py:1947-2271) keeps x, y, z, w, s,
+// the residuals and the directions in NumPy; here they stay in HBM and the
+// host only sees the scalars the loop branches on.
+namespace {
+
+constexpr int kIpmThreads = 256;
+
+int ipm_grid(const psipm_handle* h, int64_t n) {
+    return (int)std::min<int64_t>(blocks_for(n, kIpmThreads), (int64_t)std::max(1, h->num_sms) * 8);
+}
+
+void ipm_require(const psipm_handle* h) {
+    require(h->ipm.loaded, PSIPM_ERR_STATE, "IPM vectors used before psipm_ipm_load");
+}
+
+// y = M v with M in CSR (rows, ptr, idx, val); lanes per row from the mean row length
+void spmv_csr(psipm_handle* h, int64_t rows, int64_t nnz, const int* ptr, const int* idx, const double* val,
+              const double* v, double* y) {
+    const double mean = rows ? (double)nnz / (double)rows : 0.0;
+    const int grid = (int)std::min<int64_t>(std::max<int64_t>(1, rows / 8), (int64_t)h->num_sms * 16);
+    cudaStream_t st = h->stream;
+    if (mean <= 3.0)
+        LAUNCH(h, k_spmv_rows<1><<<grid, kIpmThreads, 0, st>>>(rows, ptr, idx, val, v, y));
+    else if (mean <= 12.0)
+        LAUNCH(h, k_spmv_rows<4><<<grid, kIpmThreads, 0, st>>>(rows, ptr, idx, val, v, y));
+    else if (mean <= 48.0)
+        LAUNCH(h, k_spmv_rows<8><<<grid, kIpmThreads, 0, st>>>(rows, ptr, idx, val, v, y));
+    else
+        LAUNCH(h, k_spmv_rows<32><<<grid, kIpmThreads, 0, st>>>(rows, ptr, idx, val, v, y));
+}
+
+void ipm_reset(psipm_handle* h, int nred, int nu, unsigned long long uval) {
+    LAUNCH(h, k_ipm_reset<<<1, 32, 0, h->stream>>>(h->ipm.red.p, nred, h->ipm.redu.p, nu, uval, h->ipm.flag.p));
+}
+
+unsigned long long bits_of(double v) {
+    unsigned long long b;
+    std::memcpy(&b, &v, sizeof(b));
+    return b;
+}
+
+double from_bits(unsigned long long b) {
+    double v;
+    std::memcpy(&v, &b, sizeof(v));
+    return v;
+}
+
+// A^T y into aty and A x into ax for the current iterate
+void ipm_products(psipm_handle* h) {
+    IpmStore& I = h->ipm;
+    spmv_csr(h, h->n, h->nnz, h->at_ptr.p, h->at_idx.p, h->at_val.p, I.y.p, I.aty.p);
+    spmv_csr(h, h->m, h->nnz, h->a_ptr.p, h->a_idx.p, h->a_val.p, I.x.p, I.ax.p);
+}
+
+template <typename U>
+void read_back(psipm_handle* h, U* host, const U* dev, int count) {
+    PSIPM_CUDA(cudaMemcpyAsync(host, dev, count * sizeof(U), cudaMemcpyDeviceToHost, h->stream));
+    PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+// which: 0 iterate (x, y, z, w), 1 centre (xk, yk, zk, wk), 2 direction D, 3 corrector C
+void ipm_set(IpmStore& I, int which, double*& x, double*& y, double*& z, double*& w) {
+    switch (which) {
+        case 0: x = I.x.p, y = I.y.p, z = I.z.p, w = I.w.p; break;
+        case 1: x = I.xk.p, y = I.yk.p, z = I.zk.p, w = I.wk.p; break;
+        case 2: x = I.dx.p, y = I.dy.p, z = I.dz.p, w = I.dw.p; break;
+        default: x = I.dxc.p, y = I.dyc.p, z = I.dzc.p, w = I.dwc.p; break;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int psipm_ipm_load(psipm_handle* h, const double* c, const double* b, const double* u, const uint8_t* pos,
+                   const uint8_t* box) {
+    if (!c || !b || !u || !pos || !box) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        const int64_t n = h->n, m = h->m;
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        I.c.upload(c, n, st);
+        I.b.upload(b, m, st);
+        I.u.upload(u, n, st);
+        I.pos.upload(pos, n, st);
+        I.box.upload(box, n, st);
+        for (DevBuf<double>* v : {&I.x, &I.z, &I.w, &I.s, &I.xk, &I.zk, &I.wk, &I.rd, &I.rmz, &I.rmw, &I.r1,
+                                  &I.aty, &I.dx, &I.dz, &I.dw, &I.dxc, &I.dzc, &I.dwc, &I.wref})
+            v->zero(n, st);
+        for (DevBuf<double>* v : {&I.y, &I.yk, &I.rp, &I.zero_m, &I.ax, &I.dy, &I.dyc}) v->zero(m, st);
+        I.red.zero(8, st);
+        I.redu.zero(4, st);
+        I.flag.zero(1, st);
+        I.loaded = true;
+        I.have_ref = false;
+    });
+}
+
+int psipm_ipm_put(psipm_handle* h, int32_t which, const double* x, const double* y, const double* z,
+                  const double* w) {
+    if (!x || !y || !z || !w || which < 0 || which > 3) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        double *dx, *dy, *dz, *dw;
+        ipm_set(h->ipm, which, dx, dy, dz, dw);
+        cudaStream_t st = h->stream;
+        PSIPM_CUDA(cudaMemcpyAsync(dx, x, h->n * sizeof(double), cudaMemcpyHostToDevice, st));
+        PSIPM_CUDA(cudaMemcpyAsync(dy, y, h->m * sizeof(double), cudaMemcpyHostToDevice, st));
+        PSIPM_CUDA(cudaMemcpyAsync(dz, z, h->n * sizeof(double), cudaMemcpyHostToDevice, st));
+        PSIPM_CUDA(cudaMemcpyAsync(dw, w, h->n * sizeof(double), cudaMemcpyHostToDevice, st));
+    });
+}
+
+int psipm_ipm_get(psipm_handle* h, int32_t which, double* x, double* y, double* z, double* w) {
+    if (which < 0 || which > 3) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        double *dx, *dy, *dz, *dw;
+        ipm_set(h->ipm, which, dx, dy, dz, dw);
+        copy_out(h, x, dx, h->n);
+        copy_out(h, y, dy, h->m);
+        copy_out(h, z, dz, h->n);
+        copy_out(h, w, dw, h->n);
+    });
+}
+
+int psipm_ipm_copy(psipm_handle* h, int32_t to_centre) {
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        const int g = blocks_for(std::max(h->n, h->m), kIpmThreads);
+        if (to_centre) {
+            LAUNCH(h, k_ipm_copy<<<g, kIpmThreads, 0, st>>>(h->n, h->m, I.x.p, I.y.p, I.z.p, I.w.p, I.xk.p, I.yk.p,
+                                                           I.zk.p, I.wk.p));
+        } else {
+            LAUNCH(h, k_ipm_copy<<<g, kIpmThreads, 0, st>>>(h->n, h->m, I.xk.p, I.yk.p, I.zk.p, I.wk.p, I.x.p, I.y.p,
+                                                           I.z.p, I.w.p));
+            LAUNCH(h, k_ipm_sync_box<<<blocks_for(h->n, kIpmThreads), kIpmThreads, 0, st>>>(h->n, I.x.p, I.s.p,
+                                                                                             I.u.p, I.box.p));
+        }
+    });
+}
+
+int psipm_ipm_residuals(psipm_handle* h, double rho, double delta, double* out) {
+    if (!out) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        const int64_t n = h->n, m = h->m;
+        ipm_products(h);
+        ipm_reset(h, 8, 0, 0ull);
+        LAUNCH(h, k_ipm_residual_n<<<ipm_grid(h, n), kIpmThreads, 0, st>>>(
+                      n, I.c.p, I.aty.p, I.x.p, I.z.p, I.w.p, I.xk.p, I.u.p, I.pos.p, rho, I.rd.p, I.red.p + 1));
+        LAUNCH(h, k_ipm_residual_m<<<ipm_grid(h, m), kIpmThreads, 0, st>>>(m, I.ax.p, I.b.p, I.y.p, I.yk.p, delta,
+                                                                            I.rp.p, I.red.p + 1));
+        LAUNCH(h, k_ipm_comp<<<ipm_grid(h, n), kIpmThreads, 0, st>>>(
+                      n, I.x.p, I.s.p, I.z.p, I.w.p, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0,
+                      0.0, I.pos.p, I.box.p, I.red.p));
+        read_back(h, out, I.red.p, 6);
+    });
+}
+
+int psipm_ipm_theta(psipm_handle* h, double theta_min, double theta_cap, double delta) {
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        h->theta.reserve(h->n);
+        LAUNCH(h, k_ipm_theta<<<blocks_for(h->n, kIpmThreads), kIpmThreads, 0, h->stream>>>(
+                      h->n, I.x.p, I.z.p, I.w.p, I.s.p, I.pos.p, I.box.p, theta_min, theta_cap, h->theta.p));
+        h->delta = delta;
+        compute_weights(h);
+        h->have_theta = true;
+        h->scores_valid = false;
+    });
+}
+
+int psipm_ipm_targets(psipm_handle* h, int32_t kind, const double* params) {
+    if (!params || kind < 0 || kind > 2) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        const int g = blocks_for(h->n, kIpmThreads);
+        cudaStream_t st = h->stream;
+        if (kind == 0)
+            LAUNCH(h, k_ipm_targets<<<g, kIpmThreads, 0, st>>>(h->n, I.x.p, I.s.p, I.z.p, I.w.p, params[0], I.pos.p,
+                                                              I.box.p, I.rmz.p, I.rmw.p));
+        else if (kind == 1)
+            LAUNCH(h, k_ipm_mehrotra<<<g, kIpmThreads, 0, st>>>(h->n, I.dx.p, I.dz.p, I.dw.p, params[0], I.pos.p,
+                                                               I.box.p, I.rmz.p, I.rmw.p));
+        else
+            LAUNCH(h, k_ipm_gondzio<<<g, kIpmThreads, 0, st>>>(h->n, I.x.p, I.s.p, I.z.p, I.w.p, I.dx.p, I.dz.p,
+                                                              I.dw.p, params[0], params[1], params[2], params[3],
+                                                              params[4], I.pos.p, I.box.p, I.rmz.p, I.rmw.p));
+    });
+}
+
+int psipm_ipm_newton(psipm_handle* h, int32_t corrector, double tol, int32_t maxit, int32_t variant,
+                     int32_t replacement, double gap_tolerance, double* alphas, double* betas, double* history,
+                     int32_t* finite, psipm_pcg_info* info) {
+    if (maxit < 0 || !finite) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        require(h->have_factor, PSIPM_ERR_STATE, "solve before a successful factor");
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        const int64_t n = h->n, m = h->m;
+        double* dx = corrector ? I.dxc.p : I.dx.p;
+        double* dy = corrector ? I.dyc.p : I.dy.p;
+        double* dz = corrector ? I.dzc.p : I.dz.p;
+        double* dw = corrector ? I.dwc.p : I.dw.p;
+        LAUNCH(h, k_ipm_r1<<<blocks_for(n, kIpmThreads), kIpmThreads, 0, st>>>(
+                      n, corrector ? nullptr : I.rd.p, I.rmz.p, I.rmw.p, I.x.p, I.s.p, I.pos.p, I.box.p, I.r1.p));
+        psipm_pcg_info local;
+        const double* dyd = nullptr;
+        solve_device(h, I.r1.p, corrector ? I.zero_m.p : I.rp.p, tol, maxit, variant, replacement, gap_tolerance, dx,
+                     &local, &dyd);
+        PSIPM_CUDA(cudaMemcpyAsync(dy, dyd, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        PSIPM_CUDA(cudaMemsetAsync(I.flag.p, 0, sizeof(int), st));
+        LAUNCH(h, k_ipm_dual_dirs<<<blocks_for(std::max(n, m), kIpmThreads), kIpmThreads, 0, st>>>(
+                      n, m, I.rmz.p, I.rmw.p, I.x.p, I.z.p, I.w.p, I.s.p, dx, dy, I.pos.p, I.box.p, dz, dw,
+                      I.flag.p));
+        int bad = 0;
+        PSIPM_CUDA(cudaMemcpyAsync(&bad, I.flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        copy_out(h, alphas, h->alphas.p, local.n_alpha);
+        copy_out(h, betas, h->betas.p, local.n_beta);
+        copy_out(h, history, h->history.p, local.n_history);
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        *finite = bad ? 0 : 1;
+        if (info) *info = local;
+    });
+}
+
+int psipm_ipm_steps(psipm_handle* h, int32_t with_corrector, double gamma, double* out) {
+    if (!out) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        ipm_reset(h, 0, 2, bits_of(1.0));
+        const bool c = with_corrector != 0;
+        LAUNCH(h, k_ipm_steps<<<ipm_grid(h, h->n), kIpmThreads, 0, h->stream>>>(
+                      h->n, I.x.p, I.s.p, I.z.p, I.w.p, I.dx.p, I.dz.p, I.dw.p, c ? I.dxc.p : nullptr,
+                      c ? I.dzc.p : nullptr, c ? I.dwc.p : nullptr, gamma, I.pos.p, I.box.p, I.redu.p));
+        unsigned long long b[2];
+        read_back(h, b, I.redu.p, 2);
+        out[0] = from_bits(b[0]);
+        out[1] = from_bits(b[1]);
+    });
+}
+
+int psipm_ipm_complementarity(psipm_handle* h, int32_t with_corrector, double gamma, double alpha_x, double alpha_z,
+                              double* out) {
+    if (!out) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        ipm_reset(h, 1, 0, 0ull);
+        const bool c = with_corrector != 0;
+        LAUNCH(h, k_ipm_comp<<<ipm_grid(h, h->n), kIpmThreads, 0, h->stream>>>(
+                      h->n, I.x.p, I.s.p, I.z.p, I.w.p, I.dx.p, I.dz.p, I.dw.p, c ? I.dxc.p : nullptr,
+                      c ? I.dzc.p : nullptr, c ? I.dwc.p : nullptr, gamma, alpha_x, alpha_z, I.pos.p, I.box.p,
+                      I.red.p));
+        read_back(h, out, I.red.p, 1);
+    });
+}
+
+int psipm_ipm_accept(psipm_handle* h, double gamma) {
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        LAUNCH(h, k_ipm_accept<<<blocks_for(std::max(h->n, h->m), kIpmThreads), kIpmThreads, 0, h->stream>>>(
+                      h->n, h->m, I.dx.p, I.dy.p, I.dz.p, I.dw.p, I.dxc.p, I.dyc.p, I.dzc.p, I.dwc.p, gamma));
+    });
+}
+
+int psipm_ipm_update(psipm_handle* h, double alpha_x, double alpha_z) {
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        LAUNCH(h, k_ipm_update<<<blocks_for(std::max(h->n, h->m), kIpmThreads), kIpmThreads, 0, h->stream>>>(
+                      h->n, h->m, I.x.p, I.y.p, I.z.p, I.w.p, I.s.p, I.u.p, I.box.p, I.dx.p, I.dy.p, I.dz.p, I.dw.p,
+                      alpha_x, alpha_z));
+    });
+}
+
+int psipm_ipm_metrics(psipm_handle* h, double* out) {
+    if (!out) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        LAUNCH(h, k_ipm_sync_box<<<blocks_for(h->n, kIpmThreads), kIpmThreads, 0, st>>>(h->n, I.x.p, I.s.p, I.u.p,
+                                                                                         I.box.p));
+        ipm_products(h);
+        ipm_reset(h, 4, 2, 0ull);
+        LAUNCH(h, k_ipm_outer_n<<<ipm_grid(h, h->n), kIpmThreads, 0, st>>>(h->n, I.c.p, I.aty.p, I.x.p, I.z.p, I.w.p,
+                                                                            I.s.p, I.u.p, I.pos.p, I.box.p, I.red.p,
+                                                                            I.redu.p));
+        LAUNCH(h, k_ipm_outer_m<<<ipm_grid(h, h->m), kIpmThreads, 0, st>>>(h->m, I.ax.p, I.b.p, I.y.p, I.red.p,
+                                                                            I.redu.p));
+        double sums[4];
+        unsigned long long mx[2];
+        PSIPM_CUDA(cudaMemcpyAsync(sums, I.red.p, sizeof(sums), cudaMemcpyDeviceToHost, st));
+        read_back(h, mx, I.redu.p, 2);
+        out[0] = from_bits(mx[0]);
+        out[1] = from_bits(mx[1]);
+        for (int q = 0; q < 4; ++q) out[2 + q] = sums[q];
+    });
+}
+
+int psipm_lag_reference(psipm_handle* h) {
+    return guarded(h, [&]() {
+        ipm_require(h);
+        require(h->have_theta, PSIPM_ERR_STATE, "lag reference before set_theta");
+        PSIPM_CUDA(cudaMemcpyAsync(h->ipm.wref.p, h->w.p, h->n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   h->stream));
+        h->ipm.have_ref = true;
+    });
+}
+
+int psipm_lag_ratio(psipm_handle* h, double* out) {
+    if (!out) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        require(h->have_theta && h->ipm.have_ref, PSIPM_ERR_STATE, "lag ratio without a reference");
+        IpmStore& I = h->ipm;
+        ipm_reset(h, 0, 2, bits_of(INFINITY));
+        LAUNCH(h, k_ipm_reset<<<1, 32, 0, h->stream>>>(nullptr, 0, I.redu.p, 1, 0ull, nullptr));
+        LAUNCH(h, k_lag_ratio<<<ipm_grid(h, h->n), kIpmThreads, 0, h->stream>>>(h->n, h->w.p, I.wref.p, I.redu.p,
+                                                                                 I.flag.p));
+        unsigned long long b[2];
+        int bad = 0;
+        PSIPM_CUDA(cudaMemcpyAsync(&bad, I.flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        read_back(h, b, I.redu.p, 2);
+        out[0] = bad ? INFINITY : from_bits(b[0]);
+        out[1] = bad ? 0.0 : from_bits(b[1]);
+    });
 }
 
 }  // extern "C"

@@ -112,6 +112,21 @@ SIGNATURES = {
     "psipm_normal_matvec_static": (_I32, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P]),
     "psipm_debug_apply_trace": (_I32, [_P, _P, _P, _P, _I32, _P, _P]),
     "psipm_timer_stop": (_I32, [_P, _P]),
+    "psipm_ipm_load": (_I32, [_P, _P, _P, _P, _P, _P]),
+    "psipm_ipm_put": (_I32, [_P, _I32, _P, _P, _P, _P]),
+    "psipm_ipm_get": (_I32, [_P, _I32, _P, _P, _P, _P]),
+    "psipm_ipm_copy": (_I32, [_P, _I32]),
+    "psipm_ipm_residuals": (_I32, [_P, _D, _D, _P]),
+    "psipm_ipm_theta": (_I32, [_P, _D, _D, _D]),
+    "psipm_ipm_targets": (_I32, [_P, _I32, _P]),
+    "psipm_ipm_newton": (_I32, [_P, _I32, _D, _I32, _I32, _I32, _D, _P, _P, _P, _P, _P]),
+    "psipm_ipm_steps": (_I32, [_P, _I32, _D, _P]),
+    "psipm_ipm_complementarity": (_I32, [_P, _I32, _D, _D, _D, _P]),
+    "psipm_ipm_accept": (_I32, [_P, _D]),
+    "psipm_ipm_update": (_I32, [_P, _D, _D]),
+    "psipm_ipm_metrics": (_I32, [_P, _P]),
+    "psipm_lag_reference": (_I32, [_P]),
+    "psipm_lag_ratio": (_I32, [_P, _P]),
 }
 
 _lib: Optional[ctypes.CDLL] = None

@@ -191,6 +191,90 @@ class NormalEquationsDevice:
                                          ctypes.byref(info)))
         return dx, self._result(dy, info, alphas, betas, history, res)
 
+    # -- device-resident IPM vectors (include/psipm_b200.h, psipm_ipm_*) -------
+    def ipm_load(self, c, b, u, pos, box) -> None:
+        self._ipm_data = (f64(c), f64(b), f64(u), np.ascontiguousarray(pos, dtype=np.uint8),
+                          np.ascontiguousarray(box, dtype=np.uint8))
+        c, b, u, pos, box = self._ipm_data
+        if c.shape != (self.n,) or b.shape != (self.m,) or u.shape != (self.n,) or pos.shape != (self.n,) \
+                or box.shape != (self.n,):
+            raise ValueError("LP data has the wrong dimensions")
+        self._check(self.lib.psipm_ipm_load(self.h, ptr(c), ptr(b), ptr(u), ptr(pos), ptr(box)))
+        self._scal = np.zeros(8)
+
+    # vector sets of psipm_ipm_put / psipm_ipm_get
+    ITERATE, CENTRE, DIRECTION, CORRECTOR = 0, 1, 2, 3
+
+    def ipm_put(self, which: int, x, y, z, w) -> None:
+        x, y, z, w = f64(x), f64(y), f64(z), f64(w)
+        if x.shape != (self.n,) or y.shape != (self.m,) or z.shape != (self.n,) or w.shape != (self.n,):
+            raise ValueError("vector set has the wrong dimensions")
+        self._check(self.lib.psipm_ipm_put(self.h, int(which), ptr(x), ptr(y), ptr(z), ptr(w)))
+
+    def ipm_get(self, which: int = 0):
+        x, z, w = np.empty(self.n), np.empty(self.n), np.empty(self.n)
+        y = np.empty(self.m)
+        self._check(self.lib.psipm_ipm_get(self.h, int(which), ptr(x), ptr(y), ptr(z), ptr(w)))
+        return x, y, z, w
+
+    def ipm_copy(self, to_centre: bool) -> None:
+        self._check(self.lib.psipm_ipm_copy(self.h, int(to_centre)))
+
+    def ipm_residuals(self, rho: float, delta: float) -> np.ndarray:
+        out = np.empty(6)
+        self._check(self.lib.psipm_ipm_residuals(self.h, float(rho), float(delta), ptr(out)))
+        return out
+
+    def ipm_theta(self, theta_min: float, theta_cap: float, delta: float) -> None:
+        self._check(self.lib.psipm_ipm_theta(self.h, float(theta_min), float(theta_cap), float(delta)))
+
+    def ipm_targets(self, kind: int, *params: float) -> None:
+        p = np.zeros(5)
+        p[: len(params)] = params
+        self._check(self.lib.psipm_ipm_targets(self.h, int(kind), ptr(p)))
+
+    def ipm_newton(self, corrector: bool, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100,
+                   gap_tolerance=0.1):
+        alphas = np.empty(max(1, maxit))
+        betas = np.empty(max(1, maxit))
+        history = np.empty(maxit + 2)
+        finite = ctypes.c_int32()
+        info = _lib.PcgInfo()
+        self._check(self.lib.psipm_ipm_newton(self.h, int(corrector), float(tol), int(maxit), int(variant),
+                                              int(replacement), float(gap_tolerance), ptr(alphas), ptr(betas),
+                                              ptr(history), ctypes.byref(finite), ctypes.byref(info)))
+        return bool(finite.value), self._result(None, info, alphas, betas, history, None)
+
+    def ipm_steps(self, with_corrector: bool = False, gamma: float = 0.0) -> Tuple[float, float]:
+        out = np.empty(2)
+        self._check(self.lib.psipm_ipm_steps(self.h, int(with_corrector), float(gamma), ptr(out)))
+        return float(out[0]), float(out[1])
+
+    def ipm_complementarity(self, alpha_x, alpha_z, with_corrector: bool = False, gamma: float = 0.0) -> float:
+        out = ctypes.c_double()
+        self._check(self.lib.psipm_ipm_complementarity(self.h, int(with_corrector), float(gamma), float(alpha_x),
+                                                       float(alpha_z), ctypes.byref(out)))
+        return float(out.value)
+
+    def ipm_accept(self, gamma: float) -> None:
+        self._check(self.lib.psipm_ipm_accept(self.h, float(gamma)))
+
+    def ipm_update(self, alpha_x: float, alpha_z: float) -> None:
+        self._check(self.lib.psipm_ipm_update(self.h, float(alpha_x), float(alpha_z)))
+
+    def ipm_metrics(self) -> np.ndarray:
+        out = np.empty(6)
+        self._check(self.lib.psipm_ipm_metrics(self.h, ptr(out)))
+        return out
+
+    def lag_reference(self) -> None:
+        self._check(self.lib.psipm_lag_reference(self.h))
+
+    def lag_ratio(self) -> Tuple[float, float]:
+        out = np.empty(2)
+        self._check(self.lib.psipm_lag_ratio(self.h, ptr(out)))
+        return float(out[0]), float(out[1])
+
     @staticmethod
     def _result(x, info, alphas, betas, history, res) -> PcgResult:
         return PcgResult(

@@ -505,12 +505,21 @@ def psipm_solve(lp, kkt_solver, tol=1e-6, maxit=200, inner_maxit=100, pc=3, rho=
     return sol
 
 
-def solve_standard(lp, tol=1e-8, device=0, precision=0, solver_options=None, **kwargs):
-    """Build the device KKT solver and run the PS-IPM (psipm_spectral_preconditioner.py:755-840)."""
+def solve_standard(lp, tol=1e-8, device=0, precision=0, solver_options=None, resident=True, **kwargs):
+    """Build the device KKT solver and run the PS-IPM (psipm_spectral_preconditioner.py:755-840).
+
+    ``resident=True`` runs the loop on device-resident vectors
+    (:func:`psipm_b200.ipm_device.psipm_solve_resident`); ``False`` runs this
+    module's host loop, which passes theta, r1, r2, dx and dy across the
+    KKT boundary as the reference does.
+    """
     opts = dict(solver_options or {})
     solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, device=device,
                                                    precision=precision, **opts)
     try:
+        if resident:
+            from .ipm_device import psipm_solve_resident
+            return psipm_solve_resident(lp, solver, tol=tol, **kwargs), solver
         return psipm_solve(lp, solver, tol=tol, **kwargs), solver
     except Exception:
         solver.close()

@@ -46,6 +46,21 @@ class KKTSolveError(RuntimeError):
     """Same role as psipm_active_pool.KKTSolveError (psipm_active_pool.py:553)."""
 
 
+class _Resident:
+    """Stands for a theta that already lives on the device (psipm_ipm_theta).
+
+    The device-resident IPM (ipm_device.py) passes it to ``factorize`` in place
+    of a host array; the policy then skips the host->device copy and computes
+    the lag bound on the device.
+    """
+
+    def __repr__(self) -> str:
+        return "RESIDENT"
+
+
+RESIDENT = _Resident()
+
+
 def low_rank_normal_columns(A, max_columns, min_nnz, clique_ratio):
     """Columns a Woodbury update would carry (psipm_active_pool.py:691-717)."""
     if max_columns <= 0 or A.shape[1] == 0:
@@ -260,6 +275,8 @@ class GpuStableActiveColumnPreconditioner:
         self.current_cg_tol = min(self.cg_tol_max, max(self.cg_tol, float(self.forcing_factor * normalized)))
 
     def _upload_weights(self, theta, delta) -> None:
+        if theta is RESIDENT:
+            return
         self.dev.set_theta(theta, delta)
         self.h2d_bytes += 8 * self.n
 
@@ -319,7 +336,7 @@ class GpuStableActiveColumnPreconditioner:
         self.t_fact += time.perf_counter() - t0
 
     def factorize(self, theta, delta) -> None:  # psipm_stable_preconditioner.py:397-432
-        theta = np.asarray(theta, dtype=float)
+        theta = theta if theta is RESIDENT else np.asarray(theta, dtype=float)
         self._weights = None
         self._upload_weights(theta, delta)
         poor = self._last_cg >= self.refresh_cg
@@ -386,6 +403,7 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self._reference_theta = None
         self._reference_delta = None
         self._factor_generation = 0
+        self.resident = False  # set by the device-resident IPM: lag bound from device weights
         self._poor_streak = 0
         self._last_condition = 1.0
         self._last_spectral_error = 0.0
@@ -408,7 +426,11 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self.last_result: Optional[KrylovResult] = None
 
     def set_ipm_context(self, res_d, res_p, res_n, tol) -> None:  # :230-250
-        current = max(float(res_n), float(np.linalg.norm(res_d)), float(np.linalg.norm(res_p)), TINY)
+        self.set_ipm_context_norms(float(np.linalg.norm(res_d)), float(np.linalg.norm(res_p)), res_n, tol)
+
+    def set_ipm_context_norms(self, norm_d, norm_p, res_n, tol) -> None:
+        """``set_ipm_context`` given the 2-norms of res_d and res_p."""
+        current = max(float(res_n), float(norm_d), float(norm_p), TINY)
         previous = self._nonlinear_residual
         self._previous_nonlinear_residual = previous
         self._nonlinear_residual = current
@@ -455,13 +477,20 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
     def _lag_bound(self, theta, delta) -> float:  # :396-410
         if self._reference_theta is None:
             return np.inf
-        weights = 1.0 / theta
-        ref = 1.0 / self._reference_theta
-        ratio = weights / np.maximum(ref, TINY)
-        finite = ratio[np.isfinite(ratio) & (ratio > 0.0)]
-        if finite.size != ratio.size:
-            return np.inf
-        bound = max(float(finite.max()), 1.0 / float(finite.min()))
+        if theta is RESIDENT or self.resident:
+            # max/min of w / max(w_ref, tiny) on the device (psipm_lag_ratio)
+            hi, lo = self.dev.lag_ratio()
+            if not np.isfinite(hi) or self.n == 0:
+                return np.inf
+            bound = max(hi, 1.0 / lo)
+        else:
+            weights = 1.0 / theta
+            ref = 1.0 / self._reference_theta
+            ratio = weights / np.maximum(ref, TINY)
+            finite = ratio[np.isfinite(ratio) & (ratio > 0.0)]
+            if finite.size != ratio.size:
+                return np.inf
+            bound = max(float(finite.max()), 1.0 / float(finite.min()))
         if self._reference_delta > 0.0 and delta > 0.0:
             dr = delta / self._reference_delta
             bound = max(bound, dr, 1.0 / dr)
@@ -471,6 +500,8 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
 
     def _factor_current(self, theta, delta) -> None:  # :412-418
         self._factor_numeric(theta, delta)
+        if self.resident:
+            self.dev.lag_reference()
         self.factor_age = 0
         self._reference_theta = theta
         self._reference_delta = float(delta)
@@ -478,7 +509,7 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self.preconditioner_nnz.append(self.nnz_factor)
 
     def factorize(self, theta, delta) -> None:  # :420-467
-        theta = np.asarray(theta, dtype=float)
+        theta = theta if theta is RESIDENT else np.asarray(theta, dtype=float)
         self._upload_weights(theta, delta)
         spectral_poor = (self._last_condition >= self.condition_limit
                          and self._last_cg >= max(10, int(0.8 * self.refresh_cg)))
@@ -507,6 +538,16 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
     def _pcg(self, r1, r2, tolerance):
         dx, res = self.dev.solve(r1, r2, tolerance, self.cg_maxit, _lib.PCG_SPECTRAL,
                                  self.residual_replacement, self.residual_gap_tolerance)
+        self.h2d_bytes += 8 * (self.n + self.m)
+        self.d2h_bytes += 8 * (self.n + self.m)
+        return dx, self._krylov(res)
+
+    def _pcg_resident(self, corrector, tolerance):
+        finite, res = self.dev.ipm_newton(corrector, tolerance, self.cg_maxit, _lib.PCG_SPECTRAL,
+                                          self.residual_replacement, self.residual_gap_tolerance)
+        return finite, self._krylov(res)
+
+    def _krylov(self, res) -> "KrylovResult":
         lo, hi, cond = ritz_estimate(res.alphas, res.betas)
         w = self.stagnation_window
         hist = res.history
@@ -521,11 +562,9 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self.pcg_bytes += pcg_launch_bytes(self.m, self.n, self.A.nnz, self.nnz_factor, res.iterations,
                                            res.matvecs, res.iterations + 2 + res.replacements, bv)
         self.refinement_sweeps += res.refinements
-        self.h2d_bytes += 8 * (self.n + self.m)
-        self.d2h_bytes += 8 * (self.n + self.m)
-        return dx, KrylovResult(res.x, res.info, res.iterations, res.relative_residual, float(cond),
-                                float(max(abs(lo - 1.0), abs(hi - 1.0))), None, res.replacements,
-                                res.residual_checks, bool(stagnated), res.seconds)
+        return KrylovResult(res.x, res.info, res.iterations, res.relative_residual, float(cond),
+                            float(max(abs(lo - 1.0), abs(hi - 1.0))), None, res.replacements,
+                            res.residual_checks, bool(stagnated), res.seconds)
 
     def _record_krylov(self, res: KrylovResult) -> None:  # :639-649
         self._last_cg = int(res.iterations)
@@ -539,13 +578,28 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self.stagnation_events += int(res.stagnated)
 
     def solve(self, r1, r2):  # :651-752
+        dx, res = self._solve_policy(lambda tol: self._pcg(r1, r2, tol))
+        return dx, res.solution
+
+    def solve_resident(self, corrector: bool) -> bool:
+        """``solve`` on the device-resident Newton system (psipm_ipm_newton).
+
+        ``corrector=False`` solves for D from (rd, rp, rmz, rmw), ``True`` for
+        C from (0, 0, rmz, rmw); the directions stay on the device.  Same
+        policy, statistics and ``KKTSolveError`` as :meth:`solve`; returns
+        whether every entry of the directions is finite.
+        """
+        finite, _ = self._solve_policy(lambda tol: self._pcg_resident(corrector, tol))
+        return finite
+
+    def _solve_policy(self, run):
         started = time.perf_counter()
         fb = self.t_fact
         if not self._has_factor:
             raise KKTSolveError("solve before a successful factorize")
         tol = self._linear_tolerance()
         try:
-            dx, res = self._pcg(r1, r2, tol)
+            dx, res = run(tol)
         except DeviceError as exc:
             self.cg_failures += 1
             raise KKTSolveError(str(exc)) from exc
@@ -561,7 +615,11 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
             self._refresh_core(None, self.delta, stable=True, force_backbone=res.info < 0 or res.stagnated)
             self._factor_current(self.theta, self.delta)
             self.core_sizes.append(int(self.core.size))
-            dx, res = self._pcg(r1, r2, tol)
+            try:
+                dx, res = run(tol)
+            except DeviceError as exc:
+                self.cg_failures += 1
+                raise KKTSolveError(str(exc)) from exc
             total += res.iterations
             failed = res.info != 0 or not np.isfinite(res.relative_residual) or res.relative_residual > tol
         if failed and res.relative_residual <= max(2.0 * tol, self.fail_tol):
@@ -583,10 +641,9 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
             self.t_solve += max(0.0, time.perf_counter() - started - (self.t_fact - fb))
             raise KKTSolveError(f"spectral stable-column PCG failed: info={res.info}, "
                                 f"residual={res.relative_residual:.2e}")
-        dy = res.solution
         self.n_solve += 1
         self.t_solve += max(0.0, time.perf_counter() - started - (self.t_fact - fb))
-        return dx, dy
+        return dx, res
 
 
 # ---------------------------------------------------------------------------

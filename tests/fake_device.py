@@ -17,6 +17,8 @@ from oracle import stable as OS
 from psipm_b200 import _lib
 from psipm_b200.device import DeviceError, PcgResult
 
+EPS = float(np.finfo(float).eps)
+
 
 class FakeDevice:
     def __init__(self, A):
@@ -161,6 +163,145 @@ class FakeDevice:
             res.info = forced.pop(0)
             res.relative_residual = 1.0
         return dx, res
+
+    # -- device-resident IPM vectors (psipm_ipm_*), in NumPy -----------------
+    def ipm_load(self, c, b, u, pos, box):
+        self.c, self.b, self.u = (np.array(v, dtype=float) for v in (c, b, u))
+        self.pos = np.asarray(pos, dtype=bool).copy()
+        self.box = np.asarray(box, dtype=bool).copy()
+        n, m = self.n, self.m
+        self.sets = [[np.zeros(n), np.zeros(m), np.zeros(n), np.zeros(n)] for _ in range(4)]
+        self.s = np.ones(n)
+        self.rd, self.rp = np.zeros(n), np.zeros(m)
+        self.rmz, self.rmw = np.zeros(n), np.zeros(n)
+        self.wref = None
+
+    def ipm_put(self, which, x, y, z, w):
+        self.sets[which] = [np.array(v, dtype=float) for v in (x, y, z, w)]
+
+    def ipm_get(self, which=0):
+        return tuple(v.copy() for v in self.sets[which])
+
+    def _floors(self, x):
+        s = np.ones(self.n)
+        ub = self.u[self.box]
+        q = 0.25 * ub
+        xf = np.minimum(8.0 * EPS, q)
+        sf = np.minimum(8.0 * EPS * np.maximum(1.0, ub), q)
+        x[self.box] = np.clip(x[self.box], xf, ub - sf)
+        s[self.box] = np.maximum(ub - x[self.box], sf)
+        return s
+
+    def ipm_copy(self, to_centre):
+        if to_centre:
+            self.sets[1] = [v.copy() for v in self.sets[0]]
+        else:
+            self.sets[0] = [v.copy() for v in self.sets[1]]
+            self.s = self._floors(self.sets[0][0])
+
+    def _comp(self, x, z, w, s):
+        return float(x[self.pos] @ z[self.pos] + s[self.box] @ w[self.box])
+
+    def ipm_residuals(self, rho, delta):
+        x, y, z, w = self.sets[0]
+        xk, yk = self.sets[1][0], self.sets[1][1]
+        aty = self.At @ y
+        self.rd = -(self.c - aty - z + w + rho * (x - xk))
+        self.rp = -(self.A @ x - self.b + delta * (y - yk))
+        g = self.c - aty + rho * (x - xk)
+        gp = g.copy()
+        gp[self.pos] = x[self.pos] - np.clip(x[self.pos] - g[self.pos], 0.0, self.u[self.pos])
+        return np.array([self._comp(x, z, w, self.s), gp @ gp, self.rp @ self.rp, self.rd @ self.rd,
+                         (x - xk) @ (x - xk), (y - yk) @ (y - yk)])
+
+    def ipm_theta(self, theta_min, theta_cap, delta):
+        x, _, z, w = self.sets[0]
+        t = np.full(self.n, theta_min)
+        t[self.pos] += z[self.pos] / x[self.pos]
+        t[self.box] += w[self.box] / self.s[self.box]
+        t = np.where(np.isfinite(t), t, theta_cap)
+        self.set_theta(np.clip(t, theta_min, theta_cap), delta)
+
+    def ipm_targets(self, kind, *p):
+        x, _, z, w = self.sets[0]
+        dx, _, dz, dw = self.sets[2]
+        s, pos, box = self.s, self.pos, self.box
+        if kind == 0:
+            self.rmz = np.where(pos, -x * z + p[0], 0.0)
+            self.rmw = np.where(box, -s * w + p[0], 0.0)
+        elif kind == 1:
+            self.rmz = np.where(pos, p[0] - dx * dz, 0.0)
+            self.rmw = np.where(box, p[0] + dx * dw, 0.0)
+        else:
+            ta_x, ta_z, mu_t, bmin, bmax = p
+            for prod, tgt, mask in (((x + ta_x * dx) * (z + ta_z * dz), self.rmz, pos),
+                                    ((s - ta_x * dx) * (w + ta_z * dw), self.rmw, box)):
+                corr = np.clip(prod, bmin * mu_t, bmax * mu_t) - prod
+                tgt[mask] = np.clip(corr, -bmax * mu_t, 2 * bmax * mu_t)[mask]
+
+    def ipm_newton(self, corrector, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100, gap_tolerance=0.1):
+        x, _, z, w = self.sets[0]
+        r1 = (np.zeros(self.n) if corrector else self.rd.copy())
+        r1[self.pos] += self.rmz[self.pos] / x[self.pos]
+        r1[self.box] -= self.rmw[self.box] / self.s[self.box]
+        r2 = np.zeros(self.m) if corrector else self.rp
+        dx, res = self.solve(r1, r2, tol, maxit, variant, replacement, gap_tolerance)
+        dy = res.x
+        dz = np.where(self.pos, (self.rmz - z * dx) / x, 0.0)
+        dw = np.where(self.box, (self.rmw + w * dx) / self.s, 0.0)
+        self.sets[3 if corrector else 2] = [dx, dy, dz, dw]
+        finite = all(np.isfinite(v).all() for v in (dx, dy, dz, dw))
+        return bool(finite), res
+
+    @staticmethod
+    def _step(v, d, mask):
+        neg = mask & (d < 0.0)
+        return 1.0 if not neg.any() else float(min(1.0, np.min(-v[neg] / d[neg])))
+
+    def _combined(self, with_corrector, gamma):
+        d = self.sets[2]
+        if not with_corrector:
+            return d
+        return [a + gamma * b for a, b in zip(d, self.sets[3])]
+
+    def ipm_steps(self, with_corrector=False, gamma=0.0):
+        x, _, z, w = self.sets[0]
+        dx, _, dz, dw = self._combined(with_corrector, gamma)
+        return (min(self._step(x, dx, self.pos), self._step(self.s, -dx, self.box)),
+                min(self._step(z, dz, self.pos), self._step(w, dw, self.box)))
+
+    def ipm_complementarity(self, alpha_x, alpha_z, with_corrector=False, gamma=0.0):
+        x, _, z, w = self.sets[0]
+        dx, _, dz, dw = self._combined(with_corrector, gamma)
+        return self._comp(x + alpha_x * dx, z + alpha_z * dz, w + alpha_z * dw, self.s - alpha_x * dx)
+
+    def ipm_accept(self, gamma):
+        self.sets[2] = self._combined(True, gamma)
+
+    def ipm_update(self, alpha_x, alpha_z):
+        x, y, z, w = self.sets[0]
+        dx, dy, dz, dw = self.sets[2]
+        x = x + alpha_x * dx
+        self.sets[0] = [x, y + alpha_z * dy, z + alpha_z * dz, w + alpha_z * dw]
+        s = self._floors(x)
+        self.s[self.box] = s[self.box]
+
+    def ipm_metrics(self):
+        x, y, z, w = self.sets[0]
+        self.s = self._floors(x)
+        rp = self.b - self.A @ x
+        rd = self.c - self.At @ y - z + w
+        return np.array([np.abs(rp).max(initial=0.0), np.abs(rd).max(initial=0.0), self.c @ x, self.b @ y,
+                         w[self.box] @ self.u[self.box], self._comp(x, z, w, self.s)])
+
+    def lag_reference(self):
+        self.wref = self.w.copy()
+
+    def lag_ratio(self):
+        ratio = self.w / np.maximum(self.wref, OS.TINY)
+        if not (np.isfinite(ratio) & (ratio > 0.0)).all():
+            return np.inf, 0.0
+        return float(ratio.max()), float(ratio.min())
 
     def close(self):
         pass
