@@ -43,7 +43,7 @@ void read_thresholds() {
 
 template <typename T>
 struct FactorStore {
-    DevBuf<T> ms, G, update, front, xp, yp, uvec, dscp, GT, fvec, bvec;
+    DevBuf<T> ms, G, update, front, xp, yp, uvec, dscp, GT, fvec, bvec, dinv;
 };
 
 template <typename T>
@@ -531,6 +531,7 @@ void analyse(psipm_handle* h) {
         fs.dscp.reserve(h->m);
         fs.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
         fs.bvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
+        fs.dinv.reserve((int64_t)(s.max_cols / kGB + 1) * kGB * kGB);  // D_J^T blocks of one big front
     };
     if (h->precision != PSIPM_FP64)
         reserve_factor(h->f32);
@@ -599,7 +600,17 @@ void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
         LAUNCH(h, k_extract_update<T><<<std::min(blocks_for(n2, 256), 8192), 256, 0, st>>>(
                       F, r, c, fa.update + s.update_off[sn]));
     }
-    LAUNCH(h, k_g_trsm<T><<<blocks_for(r, 32), 256, 0, st>>>(F, r, c, fa.G + s.panel_off[sn]));
+    // G = [I; L21] L11^{-1} by column blocks from the right (kernels_factor.cuh)
+    T* G = fa.G + s.panel_off[sn];
+    const int nblk = (c + kGB - 1) / kGB;
+    const size_t g_smem = 2 * kGB * (kGB + 1) * sizeof(T);
+    LAUNCH(h, k_diag_block_inv<T><<<nblk, 256, g_smem + 4 * kGB * sizeof(T), st>>>(F, r, c, fa.dinv));
+    LAUNCH(h, k_g_init<T><<<dim3((c + 31) / 32, (r + 31) / 32), dim3(32, 8), 0, st>>>(F, r, c, fa.dinv, G));
+    if (r > c)
+        LAUNCH(h, k_g_convert<T><<<blocks_for(r - c, kGB), 256, g_smem, st>>>(r, c, fa.dinv, nblk - 1, G));
+    for (int jb = nblk - 1; jb >= 1; --jb)
+        LAUNCH(h, k_g_update<T><<<dim3(blocks_for(r - jb * kGB, kGB), jb), 256, g_smem, st>>>(F, r, c, fa.dinv, jb,
+                                                                                           G));
     dim3 tgrid((c + 31) / 32, (r + 31) / 32), tblock(32, 8);
     LAUNCH(h, k_transpose_panel<T><<<tgrid, tblock, 0, st>>>(fa.G + s.panel_off[sn], r, c, fa.GT + s.panel_off[sn]));
 }
@@ -640,6 +651,7 @@ int factor_numeric(psipm_handle* h, double delta, int start_shift) {
     fa.GT = fs.GT.p;
     fa.update = fs.update.p;
     fa.front = fs.front.p;
+    fa.dinv = fs.dinv.p;
     fa.front_off = h->s_front_off.p;
     fa.fail = h->fail.p;
     require((int)h->small_ptr.size() == s.nlevels + 1 && (int)h->big_ptr.size() == s.nlevels + 1 &&
@@ -871,6 +883,12 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
                                         (int)(2 * kNB * (kNB + 1) * sizeof(double))));
         PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)(2 * kNB * (kNB + 1) * sizeof(double))));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_g_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kGB * (kGB + 1) * sizeof(double))));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_g_convert<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kGB * (kGB + 1) * sizeof(double))));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_diag_block_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)((2 * kGB * (kGB + 1) + 4 * kGB) * sizeof(double))));
         int per_sm = 0;
         PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<double, double>, kPcgThreads,
                                                                  pcg_smem()));

@@ -40,6 +40,7 @@ struct FactorArgs {
     T* GT = nullptr;  // transposed panels (c x r row-major), same offsets as G
     T* update = nullptr;
     T* front = nullptr;                  // level workspace
+    T* dinv = nullptr;                   // D_J^T blocks of the big front being factored
     const long long* front_off = nullptr;  // per supernode, within the level workspace
     int* fail = nullptr;
 };
@@ -374,82 +375,178 @@ __global__ void k_extract_update(const T* __restrict__ F, int r, int c, T* __res
     }
 }
 
-// G (row-major r x c) solves X L11 = [I_c ; L21] row-block by row-block:
-// 32 rows per CTA, column blocks of 32 from right to left.
+// G = [I_c ; L21] L11^{-1} (row-major r x c) for a big front, solving
+// X L11 = B = [I_c ; L21] by column blocks of kGB from the right:
+//   X[:, J] = B[:, J] D_J  with D_J = L11[J, J]^{-1},
+//   B[:, K] -= X[:, J] L11[J, K]  for every block K < J.
+// Rows are independent, so each step is one launch over (row tile, column
+// block) tiles of the trailing part; the tiles of block J-1 finish the step
+// by multiplying with D_{J-1}.  X[J, J] = D_J is written up front (the
+// identity rows of B only ever meet their own diagonal block), and the rows
+// of X above the diagonal block of J are zero, so step J touches rows >= 64 J.
+constexpr int kGB = 64;
+
+// D_J^T for every diagonal block J (row n holds column n of D_J), zero past c.
+// One CTA per block; thread (p, j) computes column j, the k-sums split in four.
 template <typename T>
-__global__ void __launch_bounds__(256) k_g_trsm(const T* __restrict__ F, int r, int c, T* __restrict__ G) {
-    __shared__ T Xs[32][33];
-    __shared__ T Ls[32][33];
-    __shared__ T Acc[32][33];
-    __shared__ T Ld[32][33];
+__global__ void __launch_bounds__(256) k_diag_block_inv(const T* __restrict__ F, int r, int c, T* __restrict__ DT) {
+    extern __shared__ __align__(16) unsigned char smem_d[];  // 2 * kGB * (kGB + 1) + 4 * kGB scalars
+    T(*L)[kGB + 1] = reinterpret_cast<T(*)[kGB + 1]>(smem_d);
+    T(*X)[kGB + 1] = L + kGB;
+    T(*part)[kGB] = reinterpret_cast<T(*)[kGB]>(X + kGB);
+    const int jc0 = blockIdx.x * kGB, jn = min(kGB, c - jc0);
     const int tid = threadIdx.x;
-    const int row0 = blockIdx.x * 32;
-    const int nrows = min(32, r - row0);
-    const int nblk = (c + 31) / 32;
-    const int maxrow = row0 + nrows - 1;
-    // rows < c are rows of L11^{-1}: zero right of the diagonal
-    const int last_blk = maxrow < c ? maxrow / 32 : nblk - 1;
-    // zero the blocks entirely right of the diagonal for top rows
-    for (int jb = last_blk + 1; jb < nblk; ++jb)
-        for (int q = tid; q < 32 * 32; q += blockDim.x) {
-            const int a = q / 32, j = jb * 32 + q % 32;
-            if (a < nrows && j < c) G[(long long)(row0 + a) * c + j] = (T)0;
+    for (int q = tid; q < kGB * kGB; q += blockDim.x) {
+        const int i = q % kGB, j = q / kGB;
+        L[i][j] = (i < jn && j < jn) ? (i >= j ? F[(long long)(jc0 + j) * r + jc0 + i] : (T)0) : (T)(i == j);
+        X[i][j] = 0;
+    }
+    __syncthreads();
+    const int j = tid % kGB, p = tid / kGB;
+    for (int i = 0; i < kGB; ++i) {
+        // X[i][j] = (delta_ij - sum_{k<i} L[i][k] X[k][j]) / L[i][i]; X[k][j] = 0 for k < j
+        T acc = 0;
+        for (int k = p; k < i; k += 4) acc += L[i][k] * X[k][j];
+        part[p][j] = acc;
+        __syncthreads();
+        if (p == 0 && i >= j)
+            X[i][j] = ((T)(i == j) - ((part[0][j] + part[1][j]) + (part[2][j] + part[3][j]))) / L[i][i];
+        __syncthreads();
+    }
+    T* out = DT + (long long)blockIdx.x * kGB * kGB;
+    for (int q = tid; q < kGB * kGB; q += blockDim.x) out[q] = X[q % kGB][q / kGB];  // out[n][k] = D[k][n]
+}
+
+// B into G: rows < c hold D_J on their diagonal block and zeros elsewhere,
+// rows >= c hold L21 (read from the column-major front through a tile).
+template <typename T>
+__global__ void k_g_init(const T* __restrict__ F, int r, int c, const T* __restrict__ DT, T* __restrict__ G) {
+    __shared__ T tile[32][33];
+    const int bi = blockIdx.y * 32, bj = blockIdx.x * 32;  // rows, cols of G
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int j = bj + y, i = bi + threadIdx.x;  // coalesced over rows of F's column j
+        tile[y][threadIdx.x] = (i >= c && i < r && j < c) ? F[(long long)j * r + i] : (T)0;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int i = bi + y, j = bj + threadIdx.x;
+        if (i >= r || j >= c) continue;
+        T v = tile[threadIdx.x][y];
+        if (i < c) {
+            const int bI = i / kGB, bJ = j / kGB;
+            v = (bI == bJ && i >= j) ? DT[(long long)bJ * kGB * kGB + (j % kGB) * kGB + (i % kGB)] : (T)0;
         }
-    const int tr = tid / 8, tc = (tid % 8) * 4;  // this thread: row tr, cols tc..tc+3
-    for (int jb = last_blk; jb >= 0; --jb) {
-        const int jc0 = jb * 32;
-        const int jn = min(32, c - jc0);
-        // acc = B[rows, J]
-        T acc[4];
+        G[(long long)i * c + j] = v;
+    }
+}
+
+// acc[a][u] += sum_k As[ty*4 + a][k] Bs[tx + 16 u][k]
+template <typename T>
+__device__ __forceinline__ void g_tile_product(const T (*As)[kGB + 1], const T (*Bs)[kGB + 1], int tx, int ty,
+                                               T (&acc)[4][4]) {
+#pragma unroll 4
+    for (int k = 0; k < kGB; ++k) {
+        T av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = As[ty * 4 + a][k];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) bv[u] = Bs[tx + 16 * u][k];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[a][u] += av[a] * bv[u];
+    }
+}
+
+// X[i0:i0+64, J] = acc D_J for the tile whose C values are in acc (rows >= r
+// are ignored); As and Bs are free on entry.
+template <typename T>
+__device__ __forceinline__ void g_tile_convert(T (*As)[kGB + 1], T (*Bs)[kGB + 1], const T* __restrict__ DTj,
+                                               int tx, int ty, T (&acc)[4][4], int i0, int r, int c, int jc0, int jn,
+                                               T* __restrict__ G) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) As[ty * 4 + a][tx + 16 * u] = acc[a][u];
+    for (int q = tid; q < kGB * kGB; q += blockDim.x) Bs[q / kGB][q % kGB] = DTj[q];
+    __syncthreads();
+    T x[4][4] = {};
+    g_tile_product(As, Bs, tx, ty, x);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int i = i0 + ty * 4 + a;
+        if (i >= r) continue;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int i = row0 + tr, j = jc0 + tc + u;
-            T b = 0;
-            if (tr < nrows && j < c) b = i < c ? (T)(i == j ? 1 : 0) : F[(long long)j * r + i];
-            acc[u] = b;
-        }
-        // acc -= X[rows, k] L11[k, J] over k >= jc0 + 32 (already solved)
-        for (int k0 = jc0 + 32; k0 < c; k0 += 32) {
-            __syncthreads();
-            for (int q = tid; q < 32 * 32; q += blockDim.x) {
-                const int a = q / 32, kk = q % 32;
-                const int i = row0 + a, k = k0 + kk;
-                Xs[a][kk] = (a < nrows && k < c) ? G[(long long)i * c + k] : (T)0;
-                const int j = jc0 + a;  // here a indexes the column j of the block
-                Ls[kk][a] = (j < c && k < c) ? F[(long long)j * r + k] : (T)0;  // L11[k, j]
-            }
-            __syncthreads();
-#pragma unroll 8
-            for (int kk = 0; kk < 32; ++kk) {
-                const T xv = Xs[tr][kk];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) acc[u] -= xv * Ls[kk][tc + u];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < 4; ++u) Acc[tr][tc + u] = acc[u];
-        for (int q = tid; q < 32 * 32; q += blockDim.x) {
-            const int a = q / 32, b = q % 32;  // L11[jc0+a, jc0+b]
-            Ld[a][b] = (a < jn && b < jn && a >= b) ? F[(long long)(jc0 + b) * r + (jc0 + a)] : (T)0;
-        }
-        __syncthreads();
-        // in-block back substitution, one row per thread: x_j = (acc_j - sum_{l>j} x_l L[l,j]) / L[j,j]
-        if (tid < nrows) {
-            for (int j = jn - 1; j >= 0; --j) {
-                T s = Acc[tid][j];
-                for (int l = j + 1; l < jn; ++l) s -= Acc[tid][l] * Ld[l][j];
-                Acc[tid][j] = s / Ld[j][j];
-            }
-        }
-        __syncthreads();
-        for (int q = tid; q < 32 * 32; q += blockDim.x) {
-            const int a = q / 32, b = q % 32;
-            if (a < nrows && b < jn) G[(long long)(row0 + a) * c + jc0 + b] = Acc[a][b];
+            const int n = tx + 16 * u;
+            if (n < jn) G[(long long)i * c + jc0 + n] = x[a][u];
         }
     }
 }
 
+// last column block J (of width jn): rows i0 = c.. of X[:, J] = B[:, J] D_J
+template <typename T>
+__global__ void __launch_bounds__(256) k_g_convert(int r, int c, const T* __restrict__ DT, int jb,
+                                                  T* __restrict__ G) {
+    extern __shared__ __align__(16) unsigned char smem_g[];
+    T(*As)[kGB + 1] = reinterpret_cast<T(*)[kGB + 1]>(smem_g);
+    T(*Bs)[kGB + 1] = As + kGB;
+    const int jc0 = jb * kGB, jn = min(kGB, c - jc0);
+    const int i0 = c + blockIdx.x * kGB;
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int i = i0 + ty * 4 + a;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int n = tx + 16 * u;
+            acc[a][u] = (i < r && n < jn) ? G[(long long)i * c + jc0 + n] : (T)0;
+        }
+    }
+    g_tile_convert(As, Bs, DT + (long long)jb * kGB * kGB, tx, ty, acc, i0, r, c, jc0, jn, G);
+}
+
+// step J = jb: B[rows >= 64 jb, K] -= X[., J] L11[J, K] for the column block
+// K = blockIdx.y < jb; the tiles of K = jb - 1 then convert it to X.
+template <typename T>
+__global__ void __launch_bounds__(256) k_g_update(const T* __restrict__ F, int r, int c, const T* __restrict__ DT,
+                                                 int jb, T* __restrict__ G) {
+    extern __shared__ __align__(16) unsigned char smem_g[];
+    T(*As)[kGB + 1] = reinterpret_cast<T(*)[kGB + 1]>(smem_g);  // As[row][k] = X[i0 + row, J]
+    T(*Bs)[kGB + 1] = As + kGB;                                  // Bs[n][k] = L11[J + k, K + n]
+    const int jc0 = jb * kGB, jn = min(kGB, c - jc0);
+    const int kc0 = blockIdx.y * kGB;
+    const int i0 = jc0 + blockIdx.x * kGB;
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    for (int q = tid; q < kGB * kGB; q += blockDim.x) {
+        const int a = q / kGB, k = q % kGB;
+        As[a][k] = (i0 + a < r && k < jn) ? G[(long long)(i0 + a) * c + jc0 + k] : (T)0;
+        Bs[a][k] = k < jn ? F[(long long)(kc0 + a) * r + jc0 + k] : (T)0;
+    }
+    __syncthreads();
+    T acc[4][4] = {};
+    g_tile_product(As, Bs, tx, ty, acc);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int i = i0 + ty * 4 + a;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[a][u] = i < r ? G[(long long)i * c + kc0 + tx + 16 * u] - acc[a][u] : (T)0;
+    }
+    if ((int)blockIdx.y != jb - 1) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = i0 + ty * 4 + a;
+            if (i >= r) continue;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) G[(long long)i * c + kc0 + tx + 16 * u] = acc[a][u];
+        }
+        return;
+    }
+    __syncthreads();  // As, Bs are reused by the conversion
+    g_tile_convert(As, Bs, DT + (long long)blockIdx.y * kGB * kGB, tx, ty, acc, i0, r, c, kc0, kGB, G);
+}
 
 // transposed copy of a big supernode's panel: GT (c x r, row-major) = G^T
 template <typename T>
