@@ -255,6 +255,11 @@ int psipm_timer_start(psipm_handle* h);
 int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t* stamps, int32_t cap,
                             int32_t* count, int32_t* barrier_ns);
 int psipm_timer_stop(psipm_handle* h, double* seconds);
+/* Shape of the current symbolic factor by height level (out[8 * l + .] for
+ * l < min(cap, *nlevels)): {supernodes, fused single-warp supernodes,
+ * supernodes cut into GEMV tasks, forward tasks, backward tasks,
+ * panel entries sum r*c, front rows sum r, largest r}. */
+int psipm_debug_levels(const psipm_handle* h, int64_t* out, int32_t cap, int32_t* nlevels);
 /* Kernels launched by this handle since creation (all of them are this
  * library's own kernels). */
 int64_t psipm_kernel_launches(const psipm_handle* h);

@@ -43,7 +43,7 @@ void read_thresholds() {
 
 template <typename T>
 struct FactorStore {
-    DevBuf<T> ms, G, update, front, xp, yp, uvec, dscp, GT, fvec, bvec, dinv;
+    DevBuf<T> ms, G, update, front, xp, yp, dscp, GT, fvec, dinv;
 };
 
 template <typename T>
@@ -113,13 +113,13 @@ struct psipm_handle {
     DevBuf<int> s_perm, s_iperm, s_first, s_rows, s_child_ptr, s_child_list, s_relind, s_level_sn;
     DevBuf<int> s_ent_col, s_ent_rowpos, s_ent_row, s_ent_colg, s_contrib_col;
     DevBuf<long long> s_rowptr, s_panel_off, s_update_off, s_uvec_off, s_entptr, s_ent_ptr,
-        s_diag_entry, s_fg_ptr, s_fg_idx, s_front_off;
+        s_diag_entry, s_front_off;
     DevBuf<double> s_contrib_val;
     DevBuf<int> fwd_ptr_d, bwd_ptr_d;
-    DevBuf<int4> fwd_tasks_d, bwd_tasks_d;
-    std::vector<int> fwd_ptr, bwd_ptr, fpre_ptr, bpre_ptr;
-    DevBuf<int> fpre_ptr_d, bpre_ptr_d;
-    DevBuf<int4> fpre_tasks_d, bpre_tasks_d;
+    DevBuf<FwdTask> fwd_tasks_d;
+    DevBuf<BwdTask> bwd_tasks_d;
+    std::vector<int> fwd_ptr, bwd_ptr;
+    DevBuf<int> fown_d, fdst_d;  // forward-sweep push maps (prec_apply)
     std::vector<int> solve_big_sn;        // supernodes with a transposed panel
     std::vector<int64_t> gt_off_host;
     DevBuf<long long> gt_off_d;
@@ -144,6 +144,9 @@ struct psipm_handle {
     DevBuf<double> x64, r64, rhs64, t64, norm64;  // FP64 refinement (FP32_REFINED)
     DevBuf<double> part;
     DevBuf<int> ctrl, iout;
+    DevBuf<unsigned int> gbar;  // grid barrier words of the persistent kernels
+    DevBuf<int> gbar_err;       // set when a barrier wait timed out
+    bool coop_used = false;     // a persistent kernel ran in the current entry point
     DevBuf<double> dout, alphas, betas, history;
     DevBuf<double> r1, r2, dx, dy, wr1;
 
@@ -178,6 +181,12 @@ int guarded(psipm_handle* h, F&& body) {
         PSIPM_CUDA(cudaSetDevice(h->device));
         body();
         PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+        if (h->coop_used) {
+            h->coop_used = false;
+            int timed_out = 0;
+            PSIPM_CUDA(cudaMemcpy(&timed_out, h->gbar_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+            if (timed_out) throw Failure(PSIPM_ERR_TIMEOUT, "a grid barrier wait of a persistent kernel timed out");
+        }
         return PSIPM_OK;
     } catch (const Failure& f) {
         return fail_code(h, f);
@@ -289,6 +298,25 @@ SpmvLayout spmv_layout(psipm_handle* h) {
     return s;
 }
 
+// The barrier words are cleared before every persistent launch (a timed-out
+// wait can leave the arrival count behind); the timeout flag once per entry point.
+void prepare_barrier(psipm_handle* h) {
+    h->gbar.reserve(2);
+    h->gbar_err.reserve(1);
+    PSIPM_CUDA(cudaMemsetAsync(h->gbar.p, 0, 2 * sizeof(unsigned int), h->stream));
+    if (!h->coop_used) PSIPM_CUDA(cudaMemsetAsync(h->gbar_err.p, 0, sizeof(int), h->stream));
+    h->coop_used = true;
+}
+
+GridBarrier grid_barrier(psipm_handle* h) {
+    h->gbar.reserve(2);
+    h->gbar_err.reserve(1);
+    GridBarrier b;
+    b.bar = h->gbar.p;
+    b.err = h->gbar_err.p;
+    return b;
+}
+
 FactorStore<double>& fstore(psipm_handle* h, const double*) { return h->f64; }
 FactorStore<float>& fstore(psipm_handle* h, const float*) { return h->f32; }
 PcgStore<double>& pstore(psipm_handle* h, const double*) { return h->p64; }
@@ -310,6 +338,7 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
     a.a_val = a_values(h, tag);
     a.w = weights(h, tag);
     a.delta = (T)h->delta;
+    a.gb = grid_barrier(h);
     PrecLayout<P>& pc = a.pc;
     pc.m = (int)h->m;
     FactorStore<P>& fs = fstore(h, ptag);
@@ -323,8 +352,9 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
         pc.sn_rowptr = h->s_rowptr.p;
         pc.sn_rows = h->s_rows.p;
         pc.uvec_off = h->s_uvec_off.p;
-        pc.fg_ptr = h->s_fg_ptr.p;
-        pc.fg_idx = h->s_fg_idx.p;
+        pc.fown = h->fown_d.p;
+        pc.fdst = h->fdst_d.p;
+        pc.nfront = h->sym.sn_rowptr[h->sym.ns];
         pc.nlevels = h->sym.nlevels;
         pc.fwd_ptr = h->fwd_ptr_d.p;
         pc.fwd_tasks = h->fwd_tasks_d.p;
@@ -332,13 +362,7 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
         pc.bwd_tasks = h->bwd_tasks_d.p;
         pc.xp = fs.xp.p;
         pc.yp = fs.yp.p;
-        pc.uvec = fs.uvec.p;
-        pc.fpre_ptr = h->fpre_ptr_d.p;
-        pc.fpre_tasks = h->fpre_tasks_d.p;
-        pc.bpre_ptr = h->bpre_ptr_d.p;
-        pc.bpre_tasks = h->bpre_tasks_d.p;
         pc.fvec = fs.fvec.p;
-        pc.bvec = fs.bvec.p;
         pc.GT = fs.GT.p;
         pc.gt_off = h->s_panel_off.p;
     }
@@ -375,6 +399,7 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
 size_t pcg_smem() { return (size_t)kPcgWarps * kStageChunk * sizeof(double); }  // covers float too
 
 void launch_coop(psipm_handle* h, const void* fn, void** args) {
+    prepare_barrier(h);
     dim3 grid(h->coop_blocks), block(kPcgThreads);
     PSIPM_CUDA(cudaLaunchCooperativeKernel(fn, grid, block, args, pcg_smem(), h->stream));
     ++h->launches;
@@ -418,8 +443,6 @@ void analyse(psipm_handle* h) {
     up64(h->s_entptr, s.sn_entptr);
     up64(h->s_ent_ptr, s.ent_ptr);
     up64(h->s_diag_entry, s.diag_entry);
-    up64(h->s_fg_ptr, s.fgather_ptr);
-    up64(h->s_fg_idx, s.fgather_idx);
     // entry row/col in permuted numbering (for the Jacobi scaling)
     std::vector<int> er(s.nentries), ec(s.nentries);
     for (int64_t e = 0; e < s.nentries; ++e) {
@@ -445,55 +468,82 @@ void analyse(psipm_handle* h) {
     h->front_total = fmax_total;
     h->front_off_host = foff;
     up64(h->s_front_off, foff);
-    // triangular-solve tasks per level (kernels_pcg.cuh, prec_apply):
-    // pre-phase chunks of 64 front positions, then 2-D GEMV tasks of
-    // kApplyRows rows x kApplyChunk contraction entries, all-zero blocks of
-    // the triangular L11^{-1} skipped.
-    std::vector<int4> ft, bt, fp, bp;
+    // triangular-solve tasks per level (kernels_pcg.cuh, prec_apply): fused
+    // single-warp tasks for small supernodes, 2-D GEMV tasks of kApplyRows
+    // rows x kApplyChunk contraction entries for the others (all-zero blocks
+    // of the triangular L11^{-1} skipped)
+    std::vector<FwdTask> ft;
+    std::vector<BwdTask> bt;
     h->fwd_ptr.assign(s.nlevels + 1, 0);
     h->bwd_ptr.assign(s.nlevels + 1, 0);
-    h->fpre_ptr.assign(s.nlevels + 1, 0);
-    h->bpre_ptr.assign(s.nlevels + 1, 0);
     for (int l = 0; l < s.nlevels; ++l) {
         for (int q = s.level_ptr[l]; q < s.level_ptr[l + 1]; ++q) {
-            int sn = s.level_sn[q];
-            int c = s.sn_first[sn + 1] - s.sn_first[sn];
-            int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
+            const int sn = s.level_sn[q];
+            const int first = s.sn_first[sn];
+            const int c = s.sn_first[sn + 1] - first;
+            const int r = (int)(s.sn_rowptr[sn + 1] - s.sn_rowptr[sn]);
+            FwdTask f{};
+            f.f = s.sn_rowptr[sn];
+            f.u = s.uvec_off[sn];
+            f.first = first;
+            f.c = c;
+            f.s = -1;
+            BwdTask b{};
+            b.rb = s.sn_rowptr[sn];
+            b.first = first;
+            b.c = c;
+            b.r = r;
+            b.s = -1;
             if (r <= kSmallRows && c <= 32) {
-                // whole supernode in one fused warp task (no pre-phase)
-                ft.push_back(make_int4(sn, 0, r, -1));
-                bt.push_back(make_int4(sn, 0, c, -1));
+                f.s = sn;
+                b.s = sn;
+                ft.push_back(f);
+                bt.push_back(b);
                 continue;
             }
-            for (int p0 = 0; p0 < r; p0 += 64) {
-                fp.push_back(make_int4(sn, p0, std::min(r, p0 + 64), 0));
-                bp.push_back(make_int4(sn, p0, std::min(r, p0 + 64), 0));
-            }
             for (int i0 = 0; i0 < r; i0 += kApplyRows) {
-                const int i1 = std::min(r, i0 + kApplyRows);
+                f.i0 = i0;
+                f.i1 = std::min(r, i0 + kApplyRows);
+                f.g = s.panel_off[sn] + (int64_t)i0 * c;
                 for (int j0 = 0; j0 < c; j0 += kApplyChunk) {
-                    if (i1 - 1 < c && j0 > i1 - 1) break;  // above the diagonal of L11^{-1}
-                    ft.push_back(make_int4(sn, i0, i1, j0));
+                    if (f.i1 - 1 < c && j0 > f.i1 - 1) break;  // above the diagonal of L11^{-1}
+                    f.j0 = j0;
+                    ft.push_back(f);
                 }
             }
             for (int j0 = 0; j0 < c; j0 += kApplyRows) {
-                const int j1 = std::min(c, j0 + kApplyRows);
+                b.j0 = j0;
+                b.j1 = std::min(c, j0 + kApplyRows);
+                b.g = s.panel_off[sn] + (int64_t)j0 * r;
                 for (int i0 = 0; i0 < r; i0 += kApplyChunk) {
-                    const int i1 = std::min(r, i0 + kApplyChunk);
-                    if (i1 - 1 < j0) continue;  // rows above the block's first column
-                    bt.push_back(make_int4(sn, j0, j1, i0));
+                    if (std::min(r, i0 + kApplyChunk) - 1 < j0) continue;  // rows above the block's first column
+                    b.i0 = i0;
+                    bt.push_back(b);
                 }
             }
         }
         h->fwd_ptr[l + 1] = (int)ft.size();
         h->bwd_ptr[l + 1] = (int)bt.size();
-        h->fpre_ptr[l + 1] = (int)fp.size();
-        h->bpre_ptr[l + 1] = (int)bp.size();
     }
-    h->fpre_ptr_d.upload(h->fpre_ptr, st);
-    h->bpre_ptr_d.upload(h->bpre_ptr, st);
-    h->fpre_tasks_d.upload(fp, st);
-    h->bpre_tasks_d.upload(bp, st);
+    // push targets of the forward sweep: pivot rows carry their permuted
+    // column (fown), update-vector rows their position in the parent (fdst)
+    require(s.sn_rowptr[s.ns] < (int64_t)INT32_MAX, PSIPM_ERR_UNSUPPORTED, "front rows exceed int32");
+    {
+        std::vector<int> fown(std::max<int64_t>(1, s.sn_rowptr[s.ns]), -1);
+        std::vector<int> fdst(std::max<int64_t>(1, s.uvec_off[s.ns]), -1);
+        for (int sn = 0; sn < s.ns; ++sn) {
+            const int first = s.sn_first[sn], c = s.sn_first[sn + 1] - first;
+            const int64_t rb = s.sn_rowptr[sn], r = s.sn_rowptr[sn + 1] - rb;
+            for (int q = 0; q < c; ++q) fown[rb + q] = first + q;
+            const int par = s.sn_parent[sn];
+            for (int64_t q = c; q < r; ++q) {
+                const int64_t e = s.uvec_off[sn] + (q - c);
+                fdst[e] = par >= 0 ? (int)(s.sn_rowptr[par] + s.relind[e]) : -1;
+            }
+        }
+        h->fown_d.upload(fown, st);
+        h->fdst_d.upload(fdst, st);
+    }
     // per level: fronts factored one per CTA (small) or by the multi-CTA path (big)
     h->small_ptr.assign(s.nlevels + 1, 0);
     h->big_ptr.assign(s.nlevels + 1, 0);
@@ -527,10 +577,8 @@ void analyse(psipm_handle* h) {
         fs.front.reserve(std::max<int64_t>(1, fmax_total));
         fs.xp.reserve(h->m);
         fs.yp.reserve(h->m);
-        fs.uvec.reserve(std::max<int64_t>(1, s.uvec_total));
         fs.dscp.reserve(h->m);
         fs.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
-        fs.bvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
         fs.dinv.reserve((int64_t)(s.max_cols / kGB + 1) * kGB * kGB);  // D_J^T blocks of one big front
     };
     if (h->precision != PSIPM_FP64)
@@ -1443,7 +1491,9 @@ int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t
             out.zero(1, h->stream);
             int iters = 1000;
             long long* op = out.p;
-            void* bargs[] = {&iters, &op};
+            GridBarrier gb = grid_barrier(h);
+            void* bargs[] = {&iters, &op, &gb};
+            prepare_barrier(h);
             PSIPM_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_probe, dim3(h->coop_blocks),
                                                    dim3(kPcgThreads), bargs, 0, h->stream));
             ++h->launches;
@@ -1453,6 +1503,31 @@ int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t
             *barrier_ns = (int32_t)(ns / iters);
         }
     });
+}
+
+int psipm_debug_levels(const psipm_handle* h, int64_t* out, int32_t cap, int32_t* nlevels) {
+    if (!h || !out || !nlevels || cap < 0) return PSIPM_ERR_ARGUMENT;
+    if (!h->have_symbolic) return PSIPM_ERR_STATE;
+    const Symbolic& s = h->sym;
+    *nlevels = s.nlevels;
+    for (int l = 0; l < s.nlevels && l < cap; ++l) {
+        int64_t* o = out + 8 * (int64_t)l;
+        std::memset(o, 0, 8 * sizeof(int64_t));
+        o[0] = s.level_ptr[l + 1] - s.level_ptr[l];
+        for (int q = s.level_ptr[l]; q < s.level_ptr[l + 1]; ++q) {
+            const int sn = s.level_sn[q];
+            const int64_t c = s.sn_first[sn + 1] - s.sn_first[sn];
+            const int64_t r = s.sn_rowptr[sn + 1] - s.sn_rowptr[sn];
+            if (r <= kSmallRows && c <= 32) ++o[1];
+            o[5] += r * c;
+            o[6] += r;
+            o[7] = std::max<int64_t>(o[7], r);
+        }
+        o[2] = o[0] - o[1];
+        o[3] = h->fwd_ptr[l + 1] - h->fwd_ptr[l];
+        o[4] = h->bwd_ptr[l + 1] - h->bwd_ptr[l];
+    }
+    return PSIPM_OK;
 }
 
 int psipm_timer_start(psipm_handle* h) {

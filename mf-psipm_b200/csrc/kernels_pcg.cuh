@@ -27,7 +27,7 @@ namespace cgx = cooperative_groups;
 
 constexpr int kPcgThreads = 256;
 constexpr int kPcgWarps = kPcgThreads / 32;
-constexpr int kStageChunk = 512;  // f_top staging per warp (elements)
+constexpr int kStageChunk = 64;   // per-warp staging of a small supernode's vector (elements)
 constexpr int kLongRow = 4096;    // rows with more nonzeros are split into chunks
 
 struct SpmvLayout {
@@ -47,6 +47,66 @@ struct SpmvLayout {
     int n_chunks = 0;
 };
 
+// Grid barrier of the persistent kernels (cooperative launches: every block
+// is resident).  Block leaders arrive with one acq_rel atomic on bar[0]; the
+// last one clears it and advances the generation bar[1]; the others poll
+// bar[1] with a short sleep between loads.  Without the sleep several hundred
+// leaders spinning on one word keep its L2 slice busy and slow down the
+// memory accesses of the blocks that are still working.  A wait longer than
+// kBarrierPolls polls sets *err and returns, so the kernel always ends; the
+// host clears both words before every launch and reports the flag.
+constexpr unsigned int kBarrierPolls = 1u << 24;
+constexpr unsigned int kBarrierSleepNs = 64;
+
+struct GridBarrier {
+    unsigned int* bar = nullptr;  // [0] arrivals, [1] generation
+    int* err = nullptr;
+
+    __device__ __forceinline__ void sync() const {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int gen, old;
+            asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(gen) : "l"(bar + 1) : "memory");
+            asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
+            if (old + 1 == gridDim.x) {
+                asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(bar) : "memory");
+                asm volatile("red.release.gpu.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
+            } else {
+                unsigned int cur = gen;
+                for (unsigned int polls = 0;; ++polls) {
+                    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar + 1) : "memory");
+                    if (cur != gen) break;
+                    if (polls >= kBarrierPolls) {
+                        atomicExch(err, 1);
+                        break;
+                    }
+                    __nanosleep(kBarrierSleepNs);
+                }
+            }
+        }
+        __syncthreads();
+    }
+};
+
+// Triangular-solve task records: everything a task needs sits in one
+// 48-byte record, so a warp reaches its data after a single load.
+struct __align__(16) FwdTask {
+    long long g;      // panel offset of the task's first row (G, row-major r x c)
+    long long f;      // front-vector offset of the supernode (sn_rowptr)
+    long long u;      // update-vector offset of the supernode (fdst base)
+    int first, c;     // first pivot column (permuted), pivot columns
+    int i0, i1;       // rows [i0, i1) of the supernode
+    int j0, s;        // first column of the chunk; s >= 0 marks a fused small supernode
+};
+struct __align__(16) BwdTask {
+    long long g;      // GT offset of the task's first row (GT, row-major c x r)
+    long long rb;     // sn_rowptr of the supernode
+    int first, c, r;  // first pivot column, pivot columns, front rows
+    int j0, j1;       // GT rows [j0, j1) (pivot columns of the supernode)
+    int i0;           // first front row of the chunk
+    int s, pad;       // s >= 0 marks a fused small supernode
+};
+
 template <typename T>
 struct PrecLayout {
     int m = 0;
@@ -59,28 +119,21 @@ struct PrecLayout {
     const long long* sn_rowptr = nullptr;
     const int* sn_rows = nullptr;
     const long long* uvec_off = nullptr;
-    const long long* fg_ptr = nullptr;
-    const long long* fg_idx = nullptr;
+    const int* fown = nullptr;   // per front row: permuted column of a pivot row, -1 below
+    const int* fdst = nullptr;   // per update-vector entry: the parent's front row, -1 at roots
+    long long nfront = 0;        // front rows of all supernodes
     int nlevels = 0;
     const int* fwd_ptr = nullptr;
-    const int4* fwd_tasks = nullptr;  // {sn, row0, row1, 0}
+    const FwdTask* fwd_tasks = nullptr;
     const int* bwd_ptr = nullptr;
-    const int4* bwd_tasks = nullptr;  // {sn, col0, col1, kind}
-    // big supernodes: pre-phase tasks per level that assemble the front
-    // vector (forward) / the gathered right-hand side (backward) in global memory
-    const int* fpre_ptr = nullptr;
-    const int4* fpre_tasks = nullptr;  // {sn, p0, p1, 0}
-    const int* bpre_ptr = nullptr;
-    const int4* bpre_tasks = nullptr;
-    T* fvec = nullptr;                 // indexed like sn_rows
-    T* bvec = nullptr;
+    const BwdTask* bwd_tasks = nullptr;
+    T* fvec = nullptr;                // front vectors f, indexed like sn_rows
     const T* GT = nullptr;             // transposed panels of big supernodes (c x r row-major)
     const long long* gt_off = nullptr;
     long long* trace = nullptr;  // optional: %globaltimer after every barrier of an apply
     int trace_cap = 0;
     T* xp = nullptr;
     T* yp = nullptr;
-    T* uvec = nullptr;
 };
 
 template <typename T, typename P = T>
@@ -102,6 +155,7 @@ struct PcgArgs {
     T* chunk_part = nullptr;
     double* part = nullptr;  // gridDim.x * 4
     int* ctrl = nullptr;     // [0] deadline flag
+    GridBarrier gb;
     int variant = 0;
     int maxit = 0;
     int replacement = 0;
@@ -247,181 +301,155 @@ __device__ void phase_b2(const PcgArgs<T, P>& a, int mode, int src, T beta, doub
 // (c pivot columns, r rows) stores G = [L11^{-1} ; L21 L11^{-1}] (r x c,
 // row-major) and its transpose GT (c x r, row-major), so both sweeps are
 // dense matrix-vector products over contiguous rows:
-//   forward  (levels bottom-up):  f = [b_s ; 0] + sum_children u_child
+//   forward  (levels bottom-up):  f_s = [b_s ; 0] + sum_children u_child
 //                                 x_s = G_top f_top,  u_s = f_bot - G_bot f_top
 //   backward (levels top-down):   v = [x_s ; -y(rows below)]
 //                                 y_s = G^T v
-// Per level and sweep: a pre-phase assembles f (or v) in global memory and
-// initialises the outputs, then 2-D tasks (kApplyRows rows x kApplyChunk
-// contraction entries) accumulate their partial products with atomics.
-constexpr int kApplyRows = 16;
-constexpr int kApplyChunk = 256;
+// The forward sweep pushes: every supernode adds its u_s straight into its
+// parent's f (fvec at fdst) with atomics, so a level needs no gather phase,
+// and one flat pass before the first level writes every f = [b_s ; 0] and
+// clears x, y.  The backward sweep gathers v into registers inside each task.
+// Big supernodes are cut into 2-D tasks of kApplyRows output rows x
+// kApplyChunk contraction entries; each lane holds kLaneCols entries of the
+// vector chunk and loads its kLaneCols columns of four rows at once.
+constexpr int kApplyRows = 4;
+constexpr int kApplyChunk = 128;
+constexpr int kLaneCols = kApplyChunk / 32;
 
-// Four rows against one vector by one warp: lanes stride the contraction
-// index, four independent accumulators, results in every lane.
-template <typename T>
-__device__ __forceinline__ void warp_dot4(const T* __restrict__ m0, const T* __restrict__ m1,
-                                          const T* __restrict__ m2, const T* __restrict__ m3,
-                                          const T* __restrict__ v, int b0, int b1, int b2, int b3,
-                                          int e, T (&out)[4]) {
-    const int lane = threadIdx.x & 31;
-    T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    const int lo = min(min(b0, b1), min(b2, b3));
-    for (int j = lo + lane; j < e; j += 32) {
-        const T vj = v[j];
-        if (j >= b0) s0 += m0[j] * vj;
-        if (j >= b1) s1 += m1[j] * vj;
-        if (j >= b2) s2 += m2[j] * vj;
-        if (j >= b3) s3 += m3[j] * vj;
-    }
-    out[0] = warp_sum(s0);
-    out[1] = warp_sum(s1);
-    out[2] = warp_sum(s2);
-    out[3] = warp_sum(s3);
-}
-
-// forward pre-phase: f into fvec, outputs initialised (x_s = 0, u_s = f_bot)
-template <typename P, typename IT>
-__device__ void prec_forward_pre(const PrecLayout<P>& pc, const IT* in, int4 task) {
-    const int lane = threadIdx.x & 31;
-    const int s = task.x;
-    const int first = pc.sn_first[s];
-    const int c = pc.sn_first[s + 1] - first;
-    const long long rb = pc.sn_rowptr[s];
-    for (int q = task.y + lane; q < task.z; q += 32) {
-        P f = 0;
-        if (q < c) {
-            const int k = first + q;
-            f = pc.dscp[k] * (P)in[pc.perm[k]];
-        }
-        for (long long g = pc.fg_ptr[rb + q]; g < pc.fg_ptr[rb + q + 1]; ++g) f += pc.uvec[pc.fg_idx[g]];
-        pc.fvec[rb + q] = f;
-        if (q < c)
-            pc.xp[first + q] = 0;
-        else
-            pc.uvec[pc.uvec_off[s] + q - c] = f;
-    }
-}
-
-// forward task {s, i0, i1, j0}: rows [i0, i1) of G against f[j0, j0+chunk)
+// warp sums of four values; lane k (k < 4) returns the total of v[k]
 template <typename P>
-__device__ void prec_forward_gemv(const PrecLayout<P>& pc, int4 task) {
+__device__ __forceinline__ P warp_sum4(P (&v)[4]) {
     const int lane = threadIdx.x & 31;
-    const int s = task.x, i0 = task.y, i1 = task.z, j0 = task.w;
-    const int first = pc.sn_first[s];
-    const int c = pc.sn_first[s + 1] - first;
+    // exchange halves so that each lane keeps two of the four partial sums
+    const bool hi16 = lane & 16;
+    P a0 = hi16 ? v[0] : v[2], a1 = hi16 ? v[1] : v[3];
+    P k0 = hi16 ? v[2] : v[0], k1 = hi16 ? v[3] : v[1];
+    k0 += __shfl_xor_sync(0xffffffffu, a0, 16);
+    k1 += __shfl_xor_sync(0xffffffffu, a1, 16);
+    // lanes < 16 hold rows {0,1}, lanes >= 16 rows {2,3}
+    const bool hi8 = lane & 8;
+    P s = hi8 ? k0 : k1;
+    P keep = hi8 ? k1 : k0;
+    keep += __shfl_xor_sync(0xffffffffu, s, 8);
+    // lane group (bit4, bit3) now holds row 2*bit4 + bit3
+    keep += __shfl_xor_sync(0xffffffffu, keep, 4);
+    keep += __shfl_xor_sync(0xffffffffu, keep, 2);
+    keep += __shfl_xor_sync(0xffffffffu, keep, 1);
+    // row k lives in lanes 8k .. 8k+7: bring it to lane k
+    return __shfl_sync(0xffffffffu, keep, (lane & 3) * 8);
+}
+
+// forward task: rows [i0, i1) (at most four) of G against f[j0, j0 + kApplyChunk).
+// Every lane loads a clamped in-row index and masks the product, so the
+// sixteen loads carry no branches and issue together.
+template <typename P>
+__device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t) {
+    const int lane = threadIdx.x & 31;
+    const int c = t.c, i0 = t.i0, i1 = t.i1, j0 = t.j0;
+    const P* __restrict__ G = pc.G + t.g;
+    const P* f = pc.fvec + t.f;
     const int j1 = min(c, j0 + kApplyChunk);
-    const long long rb = pc.sn_rowptr[s];
-    const P* __restrict__ Gs = pc.G + pc.panel_off[s];
-    const P* __restrict__ f = pc.fvec + rb;
-    for (int i = i0; i < i1; i += 4) {
-        const P* rows[4];
-        int end[4];
-        for (int k = 0; k < 4; ++k) {
-            const int ii = min(i + k, i1 - 1);
-            rows[k] = Gs + (long long)ii * c;
-            end[k] = i + k < i1 ? (ii < c ? min(j1, ii + 1) : j1) : j0;  // G_top is lower triangular
+    // epilogue operands of lane k < 4 (row i0 + k), loaded up front
+    const int ii = i0 + lane;
+    const bool bottom = lane < 4 && ii < i1 && ii >= c;
+    int e = -1;
+    P fb = 0;
+    if (bottom) {
+        e = pc.fdst[t.u + ii - c];
+        fb = j0 == 0 ? f[ii] : (P)0;
+    }
+    P fr[kLaneCols];
+#pragma unroll
+    for (int q = 0; q < kLaneCols; ++q) {
+        const int j = j0 + lane + 32 * q;
+        const P fv = f[min(j, c - 1)];
+        fr[q] = j < j1 ? fv : (P)0;
+    }
+    P d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int row = i0 + k;
+        // G_top is lower triangular; rows past i1 contribute nothing
+        const int jend = row < i1 ? (row < c ? min(j1, row + 1) : j1) : j0;
+        const P* __restrict__ g = G + (long long)min(k, i1 - i0 - 1) * c;
+        P acc = 0;
+#pragma unroll
+        for (int q = 0; q < kLaneCols; ++q) {
+            const int j = j0 + lane + 32 * q;
+            const P gv = g[min(j, c - 1)];
+            acc += j < jend ? gv * fr[q] : (P)0;
         }
-        // rows share the loop bound j1; entries past a row's own end are masked
-        P d[4];
-        const int lo = j0;
-        P s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        for (int j = lo + lane; j < j1; j += 32) {
-            const P fj = f[j];
-            if (j < end[0]) s0 += rows[0][j] * fj;
-            if (j < end[1]) s1 += rows[1][j] * fj;
-            if (j < end[2]) s2 += rows[2][j] * fj;
-            if (j < end[3]) s3 += rows[3][j] * fj;
-        }
-        d[0] = warp_sum(s0);
-        d[1] = warp_sum(s1);
-        d[2] = warp_sum(s2);
-        d[3] = warp_sum(s3);
-        if (lane < 4 && i + lane < i1) {
-            const int ii = i + lane;
-            const P v = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
-            if (ii < c)
-                atomicAdd(&pc.xp[first + ii], v);
-            else
-                atomicAdd(&pc.uvec[pc.uvec_off[s] + ii - c], -v);
-        }
+        d[k] = acc;
+    }
+    const P v = warp_sum4(d);
+    if (lane < 4 && ii < i1) {
+        if (ii < c)
+            atomicAdd(&pc.xp[t.first + ii], v);
+        else if (e >= 0)
+            atomicAdd(&pc.fvec[e], fb - v);  // u pushed into the parent's front vector
     }
 }
 
-// backward pre-phase: v into bvec, y_s = 0
+// backward task: GT rows [j0, j1) (at most four) against v[i0, i0 + kApplyChunk)
 template <typename P>
-__device__ void prec_backward_pre(const PrecLayout<P>& pc, int4 task) {
+__device__ void prec_backward_gemv(const PrecLayout<P>& pc, const BwdTask& t) {
     const int lane = threadIdx.x & 31;
-    const int s = task.x;
-    const int first = pc.sn_first[s];
-    const int c = pc.sn_first[s + 1] - first;
-    const long long rb = pc.sn_rowptr[s];
-    for (int q = task.y + lane; q < task.z; q += 32) {
-        pc.bvec[rb + q] = q < c ? pc.xp[first + q] : -pc.yp[pc.sn_rows[rb + q]];
-        if (q < c) pc.yp[first + q] = 0;
-    }
-}
-
-// backward task {s, j0, j1, i0}: columns [j0, j1) of G (rows of GT) against v[i0, i0+chunk)
-template <typename P>
-__device__ void prec_backward_gemv(const PrecLayout<P>& pc, int4 task) {
-    const int lane = threadIdx.x & 31;
-    const int s = task.x, j0 = task.y, j1 = task.z, i0 = task.w;
-    const int first = pc.sn_first[s];
-    const long long rb = pc.sn_rowptr[s];
-    const int r = (int)(pc.sn_rowptr[s + 1] - rb);
+    const int c = t.c, r = t.r, j0 = t.j0, j1 = t.j1, i0 = t.i0;
     const int i1 = min(r, i0 + kApplyChunk);
-    const P* __restrict__ GTs = pc.GT + pc.gt_off[s];
-    const P* __restrict__ v = pc.bvec + rb;
-    for (int j = j0; j < j1; j += 4) {
-        const P* rows[4];
-        int beg[4];
-        for (int k = 0; k < 4; ++k) {
-            const int jj = min(j + k, j1 - 1);
-            rows[k] = GTs + (long long)jj * r;
-            beg[k] = j + k < j1 ? max(i0, jj) : i1;  // G[i, j] = 0 for i < j
-        }
-        P d[4];
-        warp_dot4(rows[0], rows[1], rows[2], rows[3], v, beg[0], beg[1], beg[2], beg[3], i1, d);
-        if (lane < 4 && j + lane < j1) {
-            const P val = lane == 0 ? d[0] : lane == 1 ? d[1] : lane == 2 ? d[2] : d[3];
-            atomicAdd(&pc.yp[first + j + lane], val);
-        }
+    const P* __restrict__ GT = pc.GT + t.g;
+    P vr[kLaneCols];
+#pragma unroll
+    for (int q = 0; q < kLaneCols; ++q) {
+        const int i = i0 + lane + 32 * q;
+        vr[q] = i < i1 ? (i < c ? pc.xp[t.first + i] : -pc.yp[pc.sn_rows[t.rb + i]]) : (P)0;
     }
+    P d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int jj = j0 + k;
+        const int ibeg = jj < j1 ? max(i0, jj) : i1;  // G[i, j] = 0 for i < j
+        const P* __restrict__ g = GT + (long long)min(k, j1 - j0 - 1) * r;
+        P acc = 0;
+#pragma unroll
+        for (int q = 0; q < kLaneCols; ++q) {
+            const int i = i0 + lane + 32 * q;
+            const P gv = g[min(i, r - 1)];
+            acc += (i >= ibeg && i < i1) ? gv * vr[q] : (P)0;
+        }
+        d[k] = acc;
+    }
+    const P v = warp_sum4(d);
+    if (lane < 4 && j0 + lane < j1) atomicAdd(&pc.yp[t.first + j0 + lane], v);
 }
 
 // Small supernodes (r <= kSmallRows, c <= 32): one warp does the whole
-// supernode in one task, the vector staged in shared memory and one lane per
-// output, so no pre-phase, no shuffles and no atomics are needed.
+// supernode in one task with the vector staged in shared memory and one lane
+// per output row.
 constexpr int kSmallRows = 64;
 
-template <typename P, typename IT>
-__device__ void prec_forward_small(const PrecLayout<P>& pc, const IT* in, int s, P* fs) {
+template <typename P>
+__device__ void prec_forward_small(const PrecLayout<P>& pc, int s, P* fs) {
     const int lane = threadIdx.x & 31;
     const int first = pc.sn_first[s];
     const int c = pc.sn_first[s + 1] - first;
     const long long rb = pc.sn_rowptr[s];
     const int r = (int)(pc.sn_rowptr[s + 1] - rb);
-    for (int q = lane; q < r; q += 32) {
-        P f = 0;
-        if (q < c) {
-            const int k = first + q;
-            f = pc.dscp[k] * (P)in[pc.perm[k]];
-        }
-        for (long long g = pc.fg_ptr[rb + q]; g < pc.fg_ptr[rb + q + 1]; ++g) f += pc.uvec[pc.fg_idx[g]];
-        fs[q] = f;
-    }
+    const long long uo = pc.uvec_off[s];
+    for (int q = lane; q < r; q += 32) fs[q] = pc.fvec[rb + q];
     __syncwarp();
     const P* __restrict__ Gs = pc.G + pc.panel_off[s];
     for (int row = lane; row < r; row += 32) {
         const int jlim = row < c ? row + 1 : c;
         const P* __restrict__ g = Gs + (long long)row * c;
         P d = 0;
+#pragma unroll 8
         for (int j = 0; j < jlim; ++j) d += g[j] * fs[j];
-        if (row < c)
+        if (row < c) {
             pc.xp[first + row] = d;
-        else
-            pc.uvec[pc.uvec_off[s] + row - c] = fs[row] - d;
+        } else {
+            const int dst = pc.fdst[uo + row - c];
+            if (dst >= 0) atomicAdd(&pc.fvec[dst], fs[row] - d);
+        }
     }
     __syncwarp();
 }
@@ -438,6 +466,7 @@ __device__ void prec_backward_small(const PrecLayout<P>& pc, int s, P* fs) {
     if (lane < c) {
         const P* __restrict__ gt = pc.GT + pc.panel_off[s] + (long long)lane * r;
         P d = 0;
+#pragma unroll 8
         for (int i = lane; i < r; ++i) d += gt[i] * fs[i];
         pc.yp[first + lane] = d;
     }
@@ -448,27 +477,34 @@ __device__ void prec_backward_small(const PrecLayout<P>& pc, int s, P* fs) {
 // reduction provides it).
 template <typename P, typename IT>
 __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, double& acc_rz, P* fs,
-                           cgx::grid_group& grid) {
+                           const GridBarrier& grid) {
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gstride = gridDim.x * blockDim.x;
     int ntrace = 0;
     const bool tracer = pc.trace && blockIdx.x == 0 && threadIdx.x == 0;
     auto mark = [&]() {
         if (tracer && ntrace < pc.trace_cap) pc.trace[ntrace++] = global_ns();
     };
     mark();
+    // f = [Ds Pi in ; 0] for every supernode, x = y = 0
+    for (long long g = gtid; g < pc.nfront; g += gstride) {
+        const int k = pc.fown[g];
+        pc.fvec[g] = k >= 0 ? pc.dscp[k] * (P)in[pc.perm[k]] : (P)0;
+    }
+    for (int k = gtid; k < pc.m; k += gstride) {
+        pc.xp[k] = 0;
+        pc.yp[k] = 0;
+    }
+    grid.sync();
+    mark();
     // task kind (int4.w for fused tasks is -1): fused small supernode or 2-D GEMV
     for (int lev = 0; lev < pc.nlevels; ++lev) {
-        if (pc.fpre_ptr[lev + 1] > pc.fpre_ptr[lev]) {
-            for (int tk = pc.fpre_ptr[lev] + gwarp; tk < pc.fpre_ptr[lev + 1]; tk += nwarps)
-                prec_forward_pre(pc, in, pc.fpre_tasks[tk]);
-            grid.sync();
-            mark();
-        }
         for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps) {
-            const int4 task = pc.fwd_tasks[tk];
-            if (task.w < 0)
-                prec_forward_small(pc, in, task.x, fs);
+            const FwdTask task = pc.fwd_tasks[tk];
+            if (task.s >= 0)
+                prec_forward_small(pc, task.s, fs);
             else
                 prec_forward_gemv(pc, task);
         }
@@ -476,24 +512,16 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
         mark();
     }
     for (int lev = pc.nlevels - 1; lev >= 0; --lev) {
-        if (pc.bpre_ptr[lev + 1] > pc.bpre_ptr[lev]) {
-            for (int tk = pc.bpre_ptr[lev] + gwarp; tk < pc.bpre_ptr[lev + 1]; tk += nwarps)
-                prec_backward_pre(pc, pc.bpre_tasks[tk]);
-            grid.sync();
-            mark();
-        }
         for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps) {
-            const int4 task = pc.bwd_tasks[tk];
-            if (task.w < 0)
-                prec_backward_small(pc, task.x, fs);
+            const BwdTask task = pc.bwd_tasks[tk];
+            if (task.s >= 0)
+                prec_backward_small(pc, task.s, fs);
             else
                 prec_backward_gemv(pc, task);
         }
         grid.sync();
         mark();
     }
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gstride = gridDim.x * blockDim.x;
     for (int i = gtid; i < pc.m; i += gstride) {
         const int k = pc.iperm[i];
         const IT zi = (IT)(pc.dscp[k] * pc.yp[k]);
@@ -506,7 +534,7 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
 // the partials are written; the caller issues the barrier.
 template <typename T, typename P>
 __device__ void operator_pass(const PcgArgs<T, P>& a, const T* v, int src, T beta, int mode,
-                              double (&acc)[3], cgx::grid_group& grid) {
+                              double (&acc)[3], const GridBarrier& grid) {
     phase_a(a, v, src, beta);
     grid.sync();
     phase_b(a, mode, src, beta, acc);
@@ -518,7 +546,7 @@ __device__ void operator_pass(const PcgArgs<T, P>& a, const T* v, int src, T bet
 
 template <typename T, typename P>
 __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T, P> a) {
-    cgx::grid_group grid = cgx::this_grid();
+    const GridBarrier grid = a.gb;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double scratch[kPcgWarps + 1];
     P* fs = reinterpret_cast<P*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
@@ -775,8 +803,7 @@ done:
 }
 
 // Grid-barrier cost probe: `count` barriers, nothing else.
-__global__ void k_barrier_probe(int count, long long* out) {
-    cgx::grid_group grid = cgx::this_grid();
+__global__ void k_barrier_probe(int count, long long* out, GridBarrier grid) {
     const long long t0 = global_ns();
     for (int i = 0; i < count; ++i) grid.sync();
     if (blockIdx.x == 0 && threadIdx.x == 0) *out = global_ns() - t0;
@@ -785,7 +812,7 @@ __global__ void k_barrier_probe(int count, long long* out) {
 // Standalone preconditioner apply / operator kernels (cooperative as well)
 template <typename T, typename P>
 __global__ void __launch_bounds__(kPcgThreads, 3) k_apply(PcgArgs<T, P> a, const T* in, T* out) {
-    cgx::grid_group grid = cgx::this_grid();
+    const GridBarrier grid = a.gb;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P* fs = reinterpret_cast<P*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
     double dummy = 0.0;
@@ -795,7 +822,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_apply(PcgArgs<T, P> a, const
 // y = H v  (mode 0 with src = v copied into p first by the host)
 template <typename T, typename P>
 __global__ void __launch_bounds__(kPcgThreads, 3) k_matvec(PcgArgs<T, P> a) {
-    cgx::grid_group grid = cgx::this_grid();
+    const GridBarrier grid = a.gb;
     double acc[3] = {0.0, 0.0, 0.0};
     operator_pass(a, a.p, 0, (T)0, 0, acc, grid);
 }

@@ -735,25 +735,6 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
             }
         }
     }
-    // forward-solve gather lists
-    S.fgather_ptr.assign(S.sn_rowptr[ns] + 1, 0);
-    for (int32_t s = 0; s < ns; ++s) {
-        int32_t p = S.sn_parent[s];
-        if (p < 0) continue;
-        for (int64_t e = S.uvec_off[s]; e < S.uvec_off[s + 1]; ++e)
-            ++S.fgather_ptr[S.sn_rowptr[p] + S.relind[e] + 1];
-    }
-    for (int64_t q = 0; q < S.sn_rowptr[ns]; ++q) S.fgather_ptr[q + 1] += S.fgather_ptr[q];
-    S.fgather_idx.resize(S.fgather_ptr[S.sn_rowptr[ns]]);
-    {
-        std::vector<int64_t> f(S.fgather_ptr.begin(), S.fgather_ptr.end() - 1);
-        for (int32_t s = 0; s < ns; ++s) {  // ascending s: children in fixed order
-            int32_t p = S.sn_parent[s];
-            if (p < 0) continue;
-            for (int64_t e = S.uvec_off[s]; e < S.uvec_off[s + 1]; ++e)
-                S.fgather_idx[f[S.sn_rowptr[p] + S.relind[e]]++] = e;
-        }
-    }
     // ---- expanded product -------------------------------------------------
     struct Key {
         int64_t pos;   // global position key: (sn, col, rowpos) linearised

@@ -61,11 +61,6 @@ struct Symbolic {
     std::vector<int64_t> sn_entptr;    // ns+1 into entries
     std::vector<int64_t> diag_entry;   // m: entry index of the diagonal of permuted row i
 
-    // forward-solve gather: for each supernode s and front position p
-    // (0..r_s-1), the child update-vector entries that add into p
-    std::vector<int64_t> fgather_ptr;  // sum_s r_s + 1   (indexed by sn_rowptr)
-    std::vector<int64_t> fgather_idx;  // indices into the global update-vector array
-
     // statistics
     int64_t nnz_L = 0;        // stored entries of the supernodal L (incl. explicit zeros)
     int64_t panel_total = 0;  // sum r_s c_s

@@ -112,6 +112,7 @@ SIGNATURES = {
     "psipm_normal_matvec_static": (_I32, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P]),
     "psipm_debug_apply_trace": (_I32, [_P, _P, _P, _P, _I32, _P, _P]),
     "psipm_timer_stop": (_I32, [_P, _P]),
+    "psipm_debug_levels": (_I32, [_P, _P, _I32, _P]),
     "psipm_ipm_load": (_I32, [_P, _P, _P, _P, _P, _P]),
     "psipm_ipm_put": (_I32, [_P, _I32, _P, _P, _P, _P]),
     "psipm_ipm_get": (_I32, [_P, _I32, _P, _P, _P, _P]),
