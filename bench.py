@@ -10,10 +10,11 @@ the device in FP64.
 
 Keys of the JSON line:
 * value      seconds per LP solve with A already resident on the device
-             (CUDA events on the library's stream around K solves);
-* e2e        the same solve through the public API from host arrays:
-             handle creation (A uploaded), every per-iteration theta/r1/r2
-             upload and dx/dy download, the solution back on the host;
+             (CUDA events on the library's stream around K solves); the
+             PS-IPM loop keeps its vectors on the device (ipm_device.py);
+* e2e        the same solve through the public API from host arrays
+             (solve_standard): handle creation (A uploaded), c, b, u and the
+             starting point uploaded, the solution copied back to the host;
 * roofline   the persistent PCG kernel (k_pcg): algorithmic bytes of all
              its launches / its CUDA-event time, against the measured HBM
              copy bandwidth;
@@ -216,6 +217,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
 
     from psipm_b200 import ipm
+    from psipm_b200.ipm_device import psipm_solve_resident
     from psipm_b200.device import NormalEquationsDevice
     from psipm_b200.replicas import max_over_ranks
     from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner
@@ -227,7 +229,7 @@ def run_ours(args, rank, world, local_rank):
 
     def one_solve():
         solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev)
-        sol = ipm.psipm_solve(lp, solver, tol=args.tol)
+        sol = psipm_solve_resident(lp, solver, tol=args.tol)
         if sol.status != "optimal":
             raise RuntimeError(f"solve ended {sol.status}")
         return sol, solver
