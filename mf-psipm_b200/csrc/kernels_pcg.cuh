@@ -339,6 +339,10 @@ __device__ __forceinline__ P warp_sum4(P (&v)[4]) {
     return __shfl_sync(0xffffffffu, keep, (lane & 3) * 8);
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // forward task: rows [i0, i1) (at most four) of G against f[j0, j0 + kApplyChunk).
 // Every lane loads a clamped in-row index and masks the product, so the
 // sixteen loads carry no branches and issue together.
@@ -502,6 +506,8 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
     // task kind (int4.w for fused tasks is -1): fused small supernode or 2-D GEMV
     for (int lev = 0; lev < pc.nlevels; ++lev) {
         for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps) {
+            // the record of this warp's next task is pulled into L2 meanwhile
+            if ((threadIdx.x & 31) == 0 && tk + nwarps < pc.fwd_ptr[lev + 1]) prefetch_l2(pc.fwd_tasks + tk + nwarps);
             const FwdTask task = pc.fwd_tasks[tk];
             if (task.s >= 0)
                 prec_forward_small(pc, task.s, fs);
@@ -513,6 +519,7 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
     }
     for (int lev = pc.nlevels - 1; lev >= 0; --lev) {
         for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps) {
+            if ((threadIdx.x & 31) == 0 && tk + nwarps < pc.bwd_ptr[lev + 1]) prefetch_l2(pc.bwd_tasks + tk + nwarps);
             const BwdTask task = pc.bwd_tasks[tk];
             if (task.s >= 0)
                 prec_backward_small(pc, task.s, fs);

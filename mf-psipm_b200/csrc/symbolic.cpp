@@ -254,6 +254,13 @@ void nested_dissection(const Graph& g, int32_t leaf, std::vector<int32_t>& order
 // SIAM J. Matrix Anal. Appl. 17(4), 1996): elements absorb the elements of
 // the pivot, external degrees are bounded by the AMD approximation, and
 // indistinguishable variables are merged into supervariables by hashing.
+uint64_t mix64(uint64_t x) {  // splitmix64 finaliser
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
 void amd_order(const Graph& g, std::vector<int32_t>& order) {
     const int32_t n = g.n;
     order.clear();
@@ -264,6 +271,7 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
     std::vector<int64_t> deg(n, 0);
     std::vector<int8_t> status(n, VAR);
     std::vector<int64_t> wval(n, 0);
+    std::vector<int64_t> esize(n, 0);  // sum of nv over an element's variables
     std::vector<int32_t> wstamp(n, -1), mark(n, -1);
     for (int32_t i = 0; i < n; ++i) {
         V[i].assign(g.adj.begin() + g.xadj[i], g.adj.begin() + g.xadj[i + 1]);
@@ -293,6 +301,9 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
     int32_t mindeg = 0, tag = 0, step = 0;
     std::vector<int32_t> Lp;
     std::vector<std::pair<uint64_t, int32_t>> hashes;
+    // variables and elements share one index space (both are graph nodes)
+    std::vector<int32_t> setmark(n, 0);
+    int32_t setstamp = 0;
     while (eliminated < n) {
         while (mindeg <= n && head[mindeg] < 0) ++mindeg;
         if (mindeg > n) break;
@@ -346,17 +357,10 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
             for (int32_t e : E[i]) {
                 if (e == p) continue;
                 if (wstamp[e] != step) {
+                    // |Le| never changes while e lives: a variable leaves Le only as
+                    // a pivot (which absorbs e) or by merging into a variable of Le
                     wstamp[e] = step;
-                    std::vector<int32_t>& Le = L[e];
-                    size_t w = 0;
-                    int64_t size = 0;
-                    for (int32_t v : Le)
-                        if (status[v] == VAR) {
-                            Le[w++] = v;
-                            size += nv[v];
-                        }
-                    Le.resize(w);
-                    wval[e] = size;
+                    wval[e] = esize[e];
                 }
                 wval[e] -= nv[i];
             }
@@ -376,7 +380,9 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
             int64_t bound = deg[i] + degLp - nv[i];
             deg[i] = std::max<int64_t>(0, std::min<int64_t>({dext, bound, (int64_t)n - eliminated}));
         }
-        // supervariables: identical (V, E) among Lp
+        // supervariables: identical (V, E) among Lp.  The hash is a sum of
+        // mixed indices, so it needs no sorted lists; equal hashes are
+        // confirmed by marking one variable's lists and scanning the other's.
         hashes.clear();
         for (int32_t i : Lp) {
             std::vector<int32_t>& Ei = E[i];
@@ -384,15 +390,23 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
             for (int32_t e : Ei)
                 if (status[e] == ELEM) Ei[w++] = e;
             Ei.resize(w);
-            std::sort(Ei.begin(), Ei.end());
-            std::sort(V[i].begin(), V[i].end());
-            uint64_t h = 1469598103934665603ull;
-            for (int32_t v : V[i]) h = (h ^ (uint64_t)v) * 1099511628211ull;
-            h ^= 0x9e3779b97f4a7c15ull;
-            for (int32_t e : Ei) h = (h ^ (uint64_t)e) * 1099511628211ull;
+            uint64_t h = (uint64_t)V[i].size() * 0x9e3779b97f4a7c15ull + (uint64_t)Ei.size();
+            for (int32_t v : V[i]) h += mix64((uint64_t)v);
+            for (int32_t e : Ei) h += mix64((uint64_t)e ^ 0x5bd1e9955bd1e995ull);
             hashes.emplace_back(h, i);
         }
         std::sort(hashes.begin(), hashes.end());
+        auto same_lists = [&](int32_t i, int32_t j) {
+            if (V[i].size() != V[j].size() || E[i].size() != E[j].size()) return false;
+            ++setstamp;
+            for (int32_t v : V[i]) setmark[v] = setstamp;
+            for (int32_t e : E[i]) setmark[e] = setstamp;
+            for (int32_t v : V[j])
+                if (setmark[v] != setstamp) return false;
+            for (int32_t e : E[j])
+                if (setmark[e] != setstamp) return false;
+            return true;
+        };
         for (size_t a = 0; a < hashes.size();) {
             size_t b = a;
             while (b < hashes.size() && hashes[b].first == hashes[a].first) ++b;
@@ -402,7 +416,7 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
                 for (size_t y = x + 1; y < b; ++y) {
                     int32_t j = hashes[y].second;
                     if (status[j] != VAR) continue;
-                    if (V[i] == V[j] && E[i] == E[j]) {
+                    if (same_lists(i, j)) {
                         nv[i] += nv[j];
                         merged[i].push_back(j);
                         for (int32_t q : merged[j]) merged[i].push_back(q);
@@ -424,6 +438,7 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
             Lp.resize(w);
         }
         L[p] = Lp;
+        esize[p] = degLp;
         for (int32_t i : Lp) {
             insert(i);
             mindeg = std::min(mindeg, bucket_of(i));
@@ -538,18 +553,58 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
     permuted_lower(S.iperm, lx, la);
 
     // ---- column counts (row subtrees) -------------------------------------
-    std::vector<int64_t> cnt(m, 1);
-    std::vector<int32_t> mark(m, -1);
-    for (int32_t i = 0; i < m; ++i) {
-        mark[i] = i;
-        for (int64_t e = lx[i]; e < lx[i + 1]; ++e) {
-            int32_t k = la[e];
-            while (k != -1 && mark[k] != i) {
-                ++cnt[k];
-                mark[k] = i;
-                k = par[k];
+    // Column count of j = number of row subtrees T_i (i >= j) that contain j.
+    // Each T_i is described by weights on the tree: +1 at each of its leaves,
+    // -1 at the lowest common ancestor of consecutive leaves (in postorder) and
+    // -1 at the parent of i; the sum of the weights over the subtree of j is
+    // then 1 if j is in T_i and 0 otherwise (the skeleton method of Gilbert,
+    // Ng and Peyton, 1994).  Nodes are in postorder, so first[j] (smallest
+    // node of j's subtree) and the least common ancestors come from one pass
+    // with a union-find of the finished nodes: O(nnz(A)) instead of O(nnz(L)).
+    std::vector<int64_t> cnt(m, 0);
+    {
+        std::vector<int32_t> first(m, -1);
+        for (int32_t k = 0; k < m; ++k)
+            for (int32_t j = k; j != -1 && first[j] == -1; j = par[j]) first[j] = k;
+        // rows i > j of column j (transpose of the lower pattern)
+        std::vector<int64_t> ux(m + 1, 0);
+        for (int64_t e = 0; e < lx[m]; ++e) ++ux[la[e] + 1];
+        for (int32_t k = 0; k < m; ++k) ux[k + 1] += ux[k];
+        std::vector<int32_t> ua(lx[m]);
+        {
+            std::vector<int64_t> f(ux.begin(), ux.end() - 1);
+            for (int32_t i = 0; i < m; ++i)
+                for (int64_t e = lx[i]; e < lx[i + 1]; ++e) ua[f[la[e]]++] = i;
+        }
+        std::vector<int32_t> maxfirst(m, -1), prevleaf(m, -1), uf(m);
+        std::iota(uf.begin(), uf.end(), 0);
+        auto find = [&](int32_t u) {
+            int32_t r = u;
+            while (uf[r] != r) r = uf[r];
+            while (uf[u] != r) {
+                const int32_t nx = uf[u];
+                uf[u] = r;
+                u = nx;
+            }
+            return r;
+        };
+        auto leaf = [&](int32_t i, int32_t j) {  // is j a leaf of T_i?
+            if (first[j] <= maxfirst[i]) return;
+            maxfirst[i] = first[j];
+            ++cnt[j];
+            if (prevleaf[i] != -1) --cnt[find(prevleaf[i])];
+            prevleaf[i] = j;
+        };
+        for (int32_t j = 0; j < m; ++j) {
+            for (int64_t e = ux[j]; e < ux[j + 1]; ++e) leaf(ua[e], j);
+            leaf(j, j);  // the diagonal: T_j = {j} when j has no earlier neighbour
+            if (par[j] != -1) {
+                --cnt[par[j]];
+                uf[j] = par[j];
             }
         }
+        for (int32_t j = 0; j < m; ++j)
+            if (par[j] != -1) cnt[par[j]] += cnt[j];
     }
     std::vector<int32_t> nchild(m, 0);
     for (int32_t k = 0; k < m; ++k)
@@ -643,7 +698,7 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
     }
     S.sn_rowptr.assign(ns + 1, 0);
     std::vector<std::vector<int32_t>> rows(ns);
-    std::fill(mark.begin(), mark.end(), -1);
+    std::vector<int32_t> mark(m, -1);
     for (int32_t s = 0; s < ns; ++s) {
         int32_t f0 = S.sn_first[s], f1 = S.sn_first[s + 1];
         std::vector<int32_t>& R = rows[s];
