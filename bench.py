@@ -49,6 +49,13 @@ WORKLOAD = ("min-cost flow LP, 200x250 directed grid (both orientations) + 10% r
             "m=49,999 grounded rows, n=219,010 boxed arcs, nnz=438,005; spectral stable-column "
             "preconditioner, FP64")
 HBM_FALLBACK = 6650.0
+# DRAM traffic of k_pcg, from one ncu capture on a B200 of the 151st k_pcg launch
+# of `python bench.py --steps 1 --warmup 0 --no-cpu-baseline`:
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:k_pcg -s 150 -c 1 ...
+# read 66,833,828,096 B + written 767,213,824 B in 50.275744 ms.  The bench scales
+# this rate by its own average launch duration to give bytes per launch.
+KPCG_DRAM_BYTES_PER_S = (66_833_828_096 + 767_213_824) / 0.050275744
 
 
 def parse():
@@ -277,12 +284,16 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     achieved = pcg_b / pcg_s / 1e9 if pcg_s > 0 else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "frac": (achieved / peak) if achieved else None,
+            "traffic": (KPCG_DRAM_BYTES_PER_S * pcg_s / pcg_launches) if pcg_launches else None,
+            "traffic_note": "bytes per average k_pcg launch: the DRAM rate of one ncu-captured launch "
+                            "(dram__bytes_read.sum + dram__bytes_write.sum) x this run's mean launch time",
             "kernel": "k_pcg", "peak_source": f"{peak_kind} hbm_gbs",
             "pcg_launches": pcg_launches, "pcg_iterations": pcg_its,
             "pcg_seconds_per_step": pcg_s / args.steps,
-            "note": "the LP's operator (~10 MB) is L2-resident; the fraction of HBM peak is "
-                    "reported for completeness, the kernel is latency/barrier bound here"}
+            "note": "the operator (~10 MB) is L2-resident and the factor panels (0.6-1 GB read per "
+                    "preconditioner application) stream from HBM; the supernodal sweeps below the two "
+                    "top tree levels are latency bound, so the HBM fraction stays low"}
     line = None
     if rank == 0:
         sol0 = sols[-1]

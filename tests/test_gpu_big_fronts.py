@@ -86,3 +86,31 @@ def test_big_front_full_solve(precision, golden, big_path):
     assert sol.status == "optimal"
     ref = float(g["obj"])
     assert abs(sol.obj - ref) <= 1e-8 * abs(ref)
+
+
+def test_multi_panel_fronts_apply_is_inverse():
+    """A 60x80 network LP with every candidate column in the core: P equals H,
+    and the top fronts have ~1,100 pivot columns, so the blocked factor runs
+    many 64-column steps with their trailing updates and the column-block G
+    computation many steps of its own."""
+    from _helpers import normal_matrix
+    from psipm_b200 import synthetic
+    from psipm_b200.device import NormalEquationsDevice
+
+    lp = synthetic.grid_network(60, 80, seed=1000)
+    n = lp.A.shape[1]
+    theta = np.exp(np.random.default_rng(3).uniform(-4, 4, n))
+    delta = 1e-6
+    dev = NormalEquationsDevice(lp.A)
+    try:
+        dev.set_theta(theta, delta)
+        dev.set_core(dev.candidates)
+        shift, info = dev.factor(delta, 0)
+        assert shift == 0
+        assert info.max_front > 512, "the test must reach fronts of many column blocks"
+        H = normal_matrix(lp.A, theta, delta)
+        for seed in range(2):
+            r = np.random.default_rng(seed).standard_normal(lp.A.shape[0])
+            assert rel(dev.apply(r), spla.spsolve(H, r)) <= 1e-9
+    finally:
+        dev.close()
