@@ -48,40 +48,36 @@ struct SpmvLayout {
 };
 
 // Grid barrier of the persistent kernels (cooperative launches: every block
-// is resident).  Block leaders arrive with one acq_rel atomic on bar[0]; the
-// last one clears it and advances the generation bar[1]; the others poll
-// bar[1] with a short sleep between loads.  Without the sleep several hundred
-// leaders spinning on one word keep its L2 slice busy and slow down the
-// memory accesses of the blocks that are still working.  A wait longer than
-// kBarrierPolls polls sets *err and returns, so the kernel always ends; the
-// host clears both words before every launch and reports the flag.
+// is resident).  Each block leader adds to one arrival word with a release
+// atomic: block 0 adds 2^31 - (blocks - 1), every other block adds 1, so when
+// the last block has arrived the word has grown by exactly 2^31 and its top
+// bit has flipped, with no reset and no second word.  The leaders poll the top
+// bit with acquire loads and a short sleep between them.  Without the sleep
+// several hundred leaders spinning on one word keep its L2 slice busy and slow
+// down the memory accesses of the blocks that are still working.  A wait
+// longer than kBarrierPolls polls sets *err and returns, so the kernel always
+// ends; the host clears the word before every launch and reports the flag.
 constexpr unsigned int kBarrierPolls = 1u << 24;
 constexpr unsigned int kBarrierSleepNs = 64;
 
 struct GridBarrier {
-    unsigned int* bar = nullptr;  // [0] arrivals, [1] generation
+    unsigned int* bar = nullptr;  // [0] arrival word ([1] unused)
     int* err = nullptr;
 
     __device__ __forceinline__ void sync() const {
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned int gen, old;
-            asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(gen) : "l"(bar + 1) : "memory");
-            asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
-            if (old + 1 == gridDim.x) {
-                asm volatile("st.relaxed.gpu.u32 [%0], 0;" ::"l"(bar) : "memory");
-                asm volatile("red.release.gpu.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
-            } else {
-                unsigned int cur = gen;
-                for (unsigned int polls = 0;; ++polls) {
-                    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar + 1) : "memory");
-                    if (cur != gen) break;
-                    if (polls >= kBarrierPolls) {
-                        atomicExch(err, 1);
-                        break;
-                    }
-                    __nanosleep(kBarrierSleepNs);
+            const unsigned int add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+            unsigned int old, cur;
+            asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(add) : "memory");
+            for (unsigned int polls = 0;; ++polls) {
+                asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
+                if ((cur ^ old) & 0x80000000u) break;
+                if (polls >= kBarrierPolls) {
+                    atomicExch(err, 1);
+                    break;
                 }
+                __nanosleep(kBarrierSleepNs);
             }
         }
         __syncthreads();
