@@ -794,6 +794,7 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
     struct Key {
         int64_t pos;   // global position key: (sn, col, rowpos) linearised
         int32_t k;     // core-local column
+        int32_t s;     // supernode of the position
         double v;
     };
     // linearised front position: sn_rowptr-based column-major within the
@@ -823,7 +824,7 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
                     rp = it - sr;
                 }
                 int64_t pos = S.panel_off[s] + rp * c + (j - S.sn_first[s]);
-                keys.push_back({pos, (int32_t)t, col[a].second * col[b].second});
+                keys.push_back({pos, (int32_t)t, s, col[a].second * col[b].second});
             }
     }
     // every diagonal entry exists even without contributions
@@ -831,11 +832,24 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
         int32_t s = col2sn[i];
         int32_t c = S.sn_first[s + 1] - S.sn_first[s];
         int64_t rp = i - S.sn_first[s];
-        keys.push_back({S.panel_off[s] + rp * c + rp, -1, 0.0});
+        keys.push_back({S.panel_off[s] + rp * c + rp, -1, s, 0.0});
     }
-    std::sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) {
-        return a.pos < b.pos || (a.pos == b.pos && a.k < b.k);
-    });
+    // order by (position, column): a stable counting sort by supernode (positions
+    // of different supernodes do not interleave), then a sort inside each
+    // supernode's short run
+    {
+        std::vector<int64_t> bptr(ns + 1, 0);
+        for (const Key& q : keys) ++bptr[q.s + 1];
+        for (int32_t t = 0; t < ns; ++t) bptr[t + 1] += bptr[t];
+        std::vector<Key> sorted(keys.size());
+        {
+            std::vector<int64_t> f(bptr.begin(), bptr.end() - 1);
+            for (const Key& q : keys) sorted[f[q.s]++] = q;
+        }
+        auto less = [](const Key& a, const Key& b) { return a.pos < b.pos || (a.pos == b.pos && a.k < b.k); };
+        for (int32_t t = 0; t < ns; ++t) std::sort(sorted.begin() + bptr[t], sorted.begin() + bptr[t + 1], less);
+        keys.swap(sorted);
+    }
     // distinct positions -> entries
     S.ent_ptr.clear();
     S.contrib_col.clear();
