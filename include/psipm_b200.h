@@ -244,6 +244,23 @@ int psipm_ipm_metrics(psipm_handle* h, double* out);
 int psipm_lag_reference(psipm_handle* h);
 int psipm_lag_ratio(psipm_handle* h, double* out);
 
+/* ---- R2 MINRES fallback ---------------------------------------------------------
+ * The reference's _minres (psipm_spectral_preconditioner.py:583-637), used by
+ * solve (:717-737) when PCG broke down or stagnated: preconditioned MINRES on
+ * the augmented system [diag(theta) A^T; A -delta I] [dx; q] = [r1; r2] with
+ * the preconditioner diag(1/theta, P^{-1}) of the current factor, internal
+ * tolerance max(eps, min(tol, 1e-8)), at most three refinement sweeps on the
+ * true residual; dy = -q.  info: iterations (all sweeps), relative_residual
+ * (true, over max(1, ||[r1; r2]||)), ok = 1 when it is <= max(2 tol,
+ * fail_tol) (the reference's acceptance), info = 0 then, else maxit or -1.
+ * FP64 handles only.  psipm_ipm_minres does the same for the device-resident
+ * Newton system that psipm_ipm_newton(corrector) just failed to solve, and
+ * fills D (or C) and the dual directions like it. */
+int psipm_minres(psipm_handle* h, const double* r1, const double* r2, double tol, int32_t maxit,
+                 double fail_tol, double* dx, double* dy, psipm_pcg_info* info);
+int psipm_ipm_minres(psipm_handle* h, int32_t corrector, double tol, int32_t maxit, double fail_tol,
+                     int32_t* finite, psipm_pcg_info* info);
+
 /* ---- diagnostics ---------------------------------------------------------------- */
 /* Device-side stopwatch on the handle's stream (CUDA events): start records
  * an event; stop records a second one, waits for it and returns the elapsed

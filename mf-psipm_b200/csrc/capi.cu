@@ -51,6 +51,11 @@ struct PcgStore {
     DevBuf<T> rhs, x, r, z, p, q, t, tr, chunk_part, w, at_val, a_val;
 };
 
+// Work vectors of the MINRES fallback (n + m entries each).
+struct MinresWork {
+    DevBuf<double> x, rhs, cr, corr, r1, r2, y, v, w, w1, w2, t, dot;
+};
+
 // Device-resident PS-IPM state: LP data, iterate (x, y, z, w, s), proximal
 // centre (xk, yk, zk, wk), residuals, complementarity targets, the Newton
 // direction D = (dx, dy, dz, dw) and the corrector C = (dxc, dyc, dzc, dwc).
@@ -152,6 +157,7 @@ struct psipm_handle {
 
     // PS-IPM vectors
     IpmStore ipm;
+    MinresWork minres;
 
     // selection scratch
     DevBuf<unsigned char> flag_a, flag_b, flag_c, mand_flags;
@@ -1891,6 +1897,240 @@ int psipm_lag_ratio(psipm_handle* h, double* out) {
         read_back(h, b, I.redu.p, 2);
         out[0] = bad ? INFINITY : from_bits(b[0]);
         out[1] = bad ? 0.0 : from_bits(b[1]);
+    });
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// MINRES fallback on the augmented system (psipm_spectral_preconditioner.py:
+// 583-637): K [dx; q] = [r1; r2] with K = [diag(theta) A^T; A -delta I],
+// preconditioned by diag(1/theta, P^{-1}), three refinement sweeps on the true
+// residual; the direction is (dx, dy = -q).  The Krylov recurrences are
+// preconditioned MINRES (Paige and Saunders, 1975): every vector lives on the
+// device (n + m entries, the y part at offset n), the host keeps the scalars.
+namespace {
+
+__global__ void k_aug_finish(long long n, long long m, const double* __restrict__ theta, double delta,
+                             const double* __restrict__ v, double* __restrict__ y) {
+    // y holds [A^T v_y ; A v_x]; add theta o v_x and -delta v_y
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j < n) y[j] += theta[j] * v[j];
+    else if (j < n + m) y[j] -= delta * v[j];
+}
+
+__global__ void k_lincomb(long long len, double a, const double* __restrict__ x, double b,
+                          const double* __restrict__ y, double c, const double* __restrict__ z,
+                          double* __restrict__ out) {
+    // out = a x + b y + c z (y, z may be null)
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= len) return;
+    double v = a * x[j];
+    if (y) v += b * y[j];
+    if (z) v += c * z[j];
+    out[j] = v;
+}
+
+__global__ void k_dot(long long len, const double* __restrict__ x, const double* __restrict__ y,
+                      double* __restrict__ out) {
+    __shared__ double scratch[32];
+    double acc = 0.0;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < len;
+         j += (long long)gridDim.x * blockDim.x)
+        acc += x[j] * y[j];
+    acc = block_sum(acc, scratch);
+    if (threadIdx.x == 0) atomicAdd(out, acc);
+}
+
+struct MinresState {
+    psipm_handle* h;
+    MinresWork& W;
+    int64_t n, m, len;
+
+    void aug_matvec(const double* v, double* out) {  // out = K v
+        spmv_csr(h, n, h->nnz, h->at_ptr.p, h->at_idx.p, h->at_val.p, v + n, out);
+        spmv_csr(h, m, h->nnz, h->a_ptr.p, h->a_idx.p, h->a_val.p, v, out + n);
+        LAUNCH(h, k_aug_finish<<<blocks_for(len, kIpmThreads), kIpmThreads, 0, h->stream>>>(n, m, h->theta.p,
+                                                                                               h->delta, v, out));
+    }
+    void precondition(const double* v, double* out) {  // out = diag(1/theta, P^-1) v
+        LAUNCH(h, k_div<<<blocks_for(n, 256), 256, 0, h->stream>>>(n, v, h->theta.p, out));
+        PcgArgs<double, double> a = pcg_args<double, double>(h);
+        const double* in = v + n;
+        double* o = out + n;
+        void* args[] = {&a, (void*)&in, (void*)&o};
+        launch_coop(h, (const void*)k_apply<double, double>, args);
+    }
+    void lincomb(double a, const double* x, double b, const double* y, double c, const double* z, double* out) {
+        LAUNCH(h, k_lincomb<<<blocks_for(len, kIpmThreads), kIpmThreads, 0, h->stream>>>(len, a, x, b, y, c, z,
+                                                                                           out));
+    }
+    double dot(const double* x, const double* y) {
+        PSIPM_CUDA(cudaMemsetAsync(W.dot.p, 0, sizeof(double), h->stream));
+        LAUNCH(h, k_dot<<<ipm_grid(h, len), kIpmThreads, 0, h->stream>>>(len, x, y, W.dot.p));
+        double v = 0.0;
+        read_back(h, &v, W.dot.p, 1);
+        return v;
+    }
+
+    // preconditioned MINRES on K x = b from x = 0; returns the stop code
+    // (1, 2 converged; 6 iteration limit; -1 a preconditioner that is not
+    // positive definite) and adds the iterations to *its.
+    int minres(const double* b, double* x, double rtol, int maxit, int* its) {
+        const double eps = 2.220446049250313e-16;
+        cudaStream_t st = h->stream;
+        // the rotating vectors are pointers into fixed buffers
+        double *R1 = W.r1.p, *R2 = W.r2.p, *Wn = W.w.p, *W1 = W.w1.p, *W2 = W.w2.p;
+        PSIPM_CUDA(cudaMemsetAsync(x, 0, len * sizeof(double), st));
+        PSIPM_CUDA(cudaMemcpyAsync(R1, b, len * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        precondition(R1, W.y.p);
+        double beta1 = dot(R1, W.y.p);
+        if (beta1 < 0.0) return -1;
+        if (beta1 == 0.0) return 0;
+        beta1 = std::sqrt(beta1);
+        PSIPM_CUDA(cudaMemcpyAsync(R2, R1, len * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        PSIPM_CUDA(cudaMemsetAsync(Wn, 0, len * sizeof(double), st));
+        PSIPM_CUDA(cudaMemsetAsync(W2, 0, len * sizeof(double), st));
+        double oldb = 0.0, beta = beta1, dbar = 0.0, epsln = 0.0, phibar = beta1, cs = -1.0, sn = 0.0;
+        double tnorm2 = 0.0, ynorm2 = 0.0;
+        int istop = 6;
+        for (int itn = 1; itn <= maxit; ++itn) {
+            ++*its;
+            const double s = 1.0 / beta;
+            lincomb(s, W.y.p, 0.0, nullptr, 0.0, nullptr, W.v.p);          // v = y / beta
+            aug_matvec(W.v.p, W.y.p);                                      // y = K v
+            if (itn >= 2) lincomb(1.0, W.y.p, -beta / oldb, R1, 0.0, nullptr, W.y.p);
+            const double alfa = dot(W.v.p, W.y.p);
+            lincomb(1.0, W.y.p, -alfa / beta, R2, 0.0, nullptr, W.y.p);
+            std::swap(R1, R2);                                             // r1 = r2, r2 = y
+            PSIPM_CUDA(cudaMemcpyAsync(R2, W.y.p, len * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            precondition(R2, W.y.p);
+            oldb = beta;
+            const double b2 = dot(R2, W.y.p);
+            if (b2 < 0.0) return -1;
+            beta = std::sqrt(b2);
+            tnorm2 += alfa * alfa + oldb * oldb + beta * beta;
+            // previous rotation, then the new one
+            const double oldeps = epsln;
+            const double delta = cs * dbar + sn * alfa;
+            const double gbar = sn * dbar - cs * alfa;
+            epsln = sn * beta;
+            dbar = -cs * beta;
+            const double root = std::sqrt(gbar * gbar + dbar * dbar);
+            const double gamma = std::max(std::sqrt(gbar * gbar + beta * beta), eps);
+            cs = gbar / gamma;
+            sn = beta / gamma;
+            const double phi = cs * phibar;
+            phibar = sn * phibar;
+            // w = (v - oldeps w1 - delta w2) / gamma with (w1, w2) = (w2, w); x += phi w
+            std::swap(W1, W2);
+            std::swap(W2, Wn);
+            lincomb(1.0 / gamma, W.v.p, -oldeps / gamma, W1, -delta / gamma, W2, Wn);
+            lincomb(1.0, x, phi, Wn, 0.0, nullptr, x);
+            ynorm2 = dot(x, x);
+            const double anorm = std::sqrt(tnorm2), ynorm = std::sqrt(ynorm2);
+            const double test1 = phibar / std::max(anorm * ynorm, 1e-300);
+            const double test2 = root / std::max(anorm, 1e-300);
+            if (test2 <= rtol) istop = 2;
+            if (test1 <= rtol) istop = 1;
+            if (istop != 6) return istop;
+        }
+        return 6;
+    }
+};
+
+// the reference's _minres: refinement sweeps on the true residual
+void minres_solve(psipm_handle* h, const double* r1d, const double* r2d, double tol, int maxit, double fail_tol,
+                  double* dxd, double* dyd, psipm_pcg_info* info) {
+    const int64_t n = h->n, m = h->m, len = n + m;
+    MinresWork& W = h->minres;
+    for (DevBuf<double>* b : {&W.x, &W.rhs, &W.cr, &W.corr, &W.r1, &W.r2, &W.y, &W.v, &W.w, &W.w1, &W.w2, &W.t})
+        b->reserve(len);
+    W.dot.reserve(1);
+    MinresState S{h, W, n, m, len};
+    cudaStream_t st = h->stream;
+    PSIPM_CUDA(cudaMemcpyAsync(W.rhs.p, r1d, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    PSIPM_CUDA(cudaMemcpyAsync(W.rhs.p + n, r2d, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    PSIPM_CUDA(cudaMemsetAsync(W.x.p, 0, len * sizeof(double), st));
+    const double scale = std::max(1.0, std::sqrt(S.dot(W.rhs.p, W.rhs.p)));
+    const double target = std::max(2.0 * tol, fail_tol);
+    const double rtol = std::max(2.220446049250313e-16, std::min(tol, 1e-8));
+    int its = 0, code = maxit, stop = 0;
+    double rel = 0.0;
+    for (int sweep = 0; sweep < 3; ++sweep) {
+        S.aug_matvec(W.x.p, W.t.p);
+        S.lincomb(1.0, W.rhs.p, -1.0, W.t.p, 0.0, nullptr, W.cr.p);
+        rel = std::sqrt(S.dot(W.cr.p, W.cr.p)) / scale;
+        if (std::isfinite(rel) && rel <= target) {
+            code = 0;
+            break;
+        }
+        stop = S.minres(W.cr.p, W.corr.p, rtol, maxit, &its);
+        S.lincomb(1.0, W.x.p, 1.0, W.corr.p, 0.0, nullptr, W.x.p);
+        code = stop < 0 ? -1 : (stop == 6 ? maxit : 0);
+        if (stop < 0) break;
+    }
+    S.aug_matvec(W.x.p, W.t.p);
+    S.lincomb(1.0, W.rhs.p, -1.0, W.t.p, 0.0, nullptr, W.cr.p);
+    rel = std::sqrt(S.dot(W.cr.p, W.cr.p)) / scale;
+    const bool accepted = std::isfinite(rel) && rel <= target;
+    PSIPM_CUDA(cudaMemcpyAsync(dxd, W.x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    LAUNCH(h, k_lincomb<<<blocks_for(m, kIpmThreads), kIpmThreads, 0, st>>>(m, -1.0, W.x.p + n, 0.0, nullptr, 0.0,
+                                                                            nullptr, dyd));
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->iterations = its;
+        info->info = accepted ? 0 : code;
+        info->ok = accepted ? 1 : 0;
+        info->relative_residual = rel;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int psipm_minres(psipm_handle* h, const double* r1, const double* r2, double tol, int32_t maxit, double fail_tol,
+                 double* dx, double* dy, psipm_pcg_info* info) {
+    if (!r1 || !r2 || !dx || !dy || maxit <= 0) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_factor, PSIPM_ERR_STATE, "minres before a successful factor");
+        require(h->precision == PSIPM_FP64, PSIPM_ERR_UNSUPPORTED, "the MINRES fallback is FP64 only");
+        h->r1.upload(r1, h->n, h->stream);
+        h->r2.upload(r2, h->m, h->stream);
+        h->dx.reserve(h->n);
+        h->dy.reserve(h->m);
+        minres_solve(h, h->r1.p, h->r2.p, tol, maxit, fail_tol, h->dx.p, h->dy.p, info);
+        copy_out(h, dx, h->dx.p, h->n);
+        copy_out(h, dy, h->dy.p, h->m);
+    });
+}
+
+int psipm_ipm_minres(psipm_handle* h, int32_t corrector, double tol, int32_t maxit, double fail_tol, int32_t* finite,
+                     psipm_pcg_info* info) {
+    if (maxit <= 0 || !finite) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        require(h->have_factor, PSIPM_ERR_STATE, "minres before a successful factor");
+        require(h->precision == PSIPM_FP64, PSIPM_ERR_UNSUPPORTED, "the MINRES fallback is FP64 only");
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        const int64_t n = h->n, m = h->m;
+        double* dx = corrector ? I.dxc.p : I.dx.p;
+        double* dy = corrector ? I.dyc.p : I.dy.p;
+        double* dz = corrector ? I.dzc.p : I.dz.p;
+        double* dw = corrector ? I.dwc.p : I.dw.p;
+        // r1 as the preceding psipm_ipm_newton built it
+        LAUNCH(h, k_ipm_r1<<<blocks_for(n, kIpmThreads), kIpmThreads, 0, st>>>(
+                      n, corrector ? nullptr : I.rd.p, I.rmz.p, I.rmw.p, I.x.p, I.s.p, I.pos.p, I.box.p, I.r1.p));
+        minres_solve(h, I.r1.p, corrector ? I.zero_m.p : I.rp.p, tol, maxit, fail_tol, dx, dy, info);
+        PSIPM_CUDA(cudaMemsetAsync(I.flag.p, 0, sizeof(int), st));
+        LAUNCH(h, k_ipm_dual_dirs<<<blocks_for(std::max(n, m), kIpmThreads), kIpmThreads, 0, st>>>(
+                      n, m, I.rmz.p, I.rmw.p, I.x.p, I.z.p, I.w.p, I.s.p, dx, dy, I.pos.p, I.box.p, dz, dw,
+                      I.flag.p));
+        int bad = 0;
+        read_back(h, &bad, I.flag.p, 1);
+        *finite = bad ? 0 : 1;
     });
 }
 

@@ -128,6 +128,8 @@ SIGNATURES = {
     "psipm_ipm_metrics": (_I32, [_P, _P]),
     "psipm_lag_reference": (_I32, [_P]),
     "psipm_lag_ratio": (_I32, [_P, _P]),
+    "psipm_minres": (_I32, [_P, _P, _P, _D, _I32, _D, _P, _P, _P]),
+    "psipm_ipm_minres": (_I32, [_P, _I32, _D, _I32, _D, _P, _P]),
 }
 
 _lib: Optional[ctypes.CDLL] = None

@@ -275,6 +275,24 @@ class NormalEquationsDevice:
         self._check(self.lib.psipm_lag_ratio(self.h, ptr(out)))
         return float(out[0]), float(out[1])
 
+    # -- R2 MINRES fallback (psipm_minres / psipm_ipm_minres) ------------------
+    def minres(self, r1, r2, tol, maxit, fail_tol):
+        """(dx, dy, accepted, iterations, relative residual) of the augmented MINRES."""
+        r1, r2 = f64(r1), f64(r2)
+        dx, dy = np.empty(self.n), np.empty(self.m)
+        info = _lib.PcgInfo()
+        self._check(self.lib.psipm_minres(self.h, ptr(r1), ptr(r2), float(tol), int(maxit), float(fail_tol),
+                                          ptr(dx), ptr(dy), ctypes.byref(info)))
+        return dx, dy, bool(info.ok), int(info.iterations), float(info.relative_residual)
+
+    def ipm_minres(self, corrector: bool, tol, maxit, fail_tol):
+        """(finite, accepted, iterations, relative residual); the directions stay on the device."""
+        finite = ctypes.c_int32()
+        info = _lib.PcgInfo()
+        self._check(self.lib.psipm_ipm_minres(self.h, int(corrector), float(tol), int(maxit), float(fail_tol),
+                                              ctypes.byref(finite), ctypes.byref(info)))
+        return bool(finite.value), bool(info.ok), int(info.iterations), float(info.relative_residual)
+
     @staticmethod
     def _result(x, info, alphas, betas, history, res) -> PcgResult:
         return PcgResult(

@@ -578,8 +578,17 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self.stagnation_events += int(res.stagnated)
 
     def solve(self, r1, r2):  # :651-752
-        dx, res = self._solve_policy(lambda tol: self._pcg(r1, r2, tol))
-        return dx, res.solution
+        def fallback(tol):  # augmented MINRES (:583-637) on the device
+            dx, dy, accepted, its, rel = self.dev.minres(r1, r2, tol, self.minres_maxit, self.fail_tol)
+            self.h2d_bytes += 8 * (self.n + self.m)
+            self.d2h_bytes += 8 * (self.n + self.m)
+            return (dx, dy), accepted, its, rel
+
+        return self._solve_policy(lambda tol: self._pcg(r1, r2, tol), lambda dx, res: (dx, res.solution),
+                                  fallback if self._minres_available() else None)
+
+    def _minres_available(self) -> bool:
+        return self.precision == _lib.FP64 and hasattr(self.dev, "minres")
 
     def solve_resident(self, corrector: bool) -> bool:
         """``solve`` on the device-resident Newton system (psipm_ipm_newton).
@@ -589,10 +598,14 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         policy, statistics and ``KKTSolveError`` as :meth:`solve`; returns
         whether every entry of the directions is finite.
         """
-        finite, _ = self._solve_policy(lambda tol: self._pcg_resident(corrector, tol))
-        return finite
+        def fallback(tol):
+            finite, accepted, its, rel = self.dev.ipm_minres(corrector, tol, self.minres_maxit, self.fail_tol)
+            return finite, accepted, its, rel
 
-    def _solve_policy(self, run):
+        return self._solve_policy(lambda tol: self._pcg_resident(corrector, tol), lambda finite, res: finite,
+                                  fallback if self._minres_available() else None)
+
+    def _solve_policy(self, run, finish, fallback=None):
         started = time.perf_counter()
         fb = self.t_fact
         if not self._has_factor:
@@ -633,17 +646,32 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         elif res.info > 0:
             self.krylov_iteration_limits += 1
         if failed:
-            # The reference falls back to preconditioned MINRES on the augmented
-            # system here when n+m <= minres_max_dimension (:717-737); the device
-            # build reports the failure instead and the IPM's regularisation
-            # retry takes over (psipm_active_pool.py:2066-2073).
+            if (fallback is not None and self.minres_fallback and self.n + self.m <= self.minres_max_dimension
+                    and (res.info < 0 or res.stagnated)):  # :717-737
+                self.cg_failures += 1
+                self.minres_fallbacks += 1
+                try:
+                    result, accepted, its, rel = fallback(tol)
+                except DeviceError as exc:
+                    self.t_solve += max(0.0, time.perf_counter() - started - (self.t_fact - fb))
+                    raise KKTSolveError(str(exc)) from exc
+                self.minres_iterations += its
+                self.full_fallbacks += 1
+                if not accepted:
+                    self.t_solve += max(0.0, time.perf_counter() - started - (self.t_fact - fb))
+                    raise KKTSolveError("spectral PCG and augmented MINRES failed: "
+                                        f"pcg info={res.info}, pcg residual={res.relative_residual:.2e}, "
+                                        f"minres residual={rel:.2e}")
+                self.n_solve += 1
+                self.t_solve += max(0.0, time.perf_counter() - started - (self.t_fact - fb))
+                return result
             self.cg_failures += 1
             self.t_solve += max(0.0, time.perf_counter() - started - (self.t_fact - fb))
             raise KKTSolveError(f"spectral stable-column PCG failed: info={res.info}, "
                                 f"residual={res.relative_residual:.2e}")
         self.n_solve += 1
         self.t_solve += max(0.0, time.perf_counter() - started - (self.t_fact - fb))
-        return dx, res
+        return finish(dx, res)
 
 
 # ---------------------------------------------------------------------------

@@ -164,6 +164,48 @@ class FakeDevice:
             res.relative_residual = 1.0
         return dx, res
 
+    # -- MINRES fallback (psipm_minres): the reference's _minres with SciPy ----
+    def minres(self, r1, r2, tol, maxit, fail_tol):
+        self._maybe_fail("minres")
+        n, m = self.n, self.m
+
+        def matvec(v):
+            return np.concatenate([self.theta * v[:n] + self.At @ v[n:], self.A @ v[:n] - self.delta * v[n:]])
+
+        def precondition(v):
+            return np.concatenate([v[:n] / self.theta, self.apply(v[n:])])
+
+        K = spla.LinearOperator((n + m, n + m), matvec=matvec, dtype=float)
+        M = spla.LinearOperator((n + m, n + m), matvec=precondition, dtype=float)
+        rhs = np.concatenate([r1, r2])
+        scale = max(1.0, float(np.linalg.norm(rhs)))
+        target = max(2.0 * tol, fail_tol)
+        x = np.zeros(n + m)
+        its = [0]
+        for _ in range(3):
+            cr = rhs - matvec(x)
+            if np.linalg.norm(cr) / scale <= target:
+                break
+            corr, info = spla.minres(K, cr, M=M, rtol=max(EPS, min(tol, 1e-8)), maxiter=maxit,
+                                     callback=lambda _: its.__setitem__(0, its[0] + 1))
+            x += corr
+            if info < 0:
+                break
+        rel = float(np.linalg.norm(rhs - matvec(x)) / scale)
+        return x[:n].copy(), -x[n:], bool(np.isfinite(rel) and rel <= target), its[0], rel
+
+    def ipm_minres(self, corrector, tol, maxit, fail_tol):
+        x, _, z, w = self.sets[0]
+        r1 = np.zeros(self.n) if corrector else self.rd.copy()
+        r1[self.pos] += self.rmz[self.pos] / x[self.pos]
+        r1[self.box] -= self.rmw[self.box] / self.s[self.box]
+        r2 = np.zeros(self.m) if corrector else self.rp
+        dx, dy, accepted, its, rel = self.minres(r1, r2, tol, maxit, fail_tol)
+        dz = np.where(self.pos, (self.rmz - z * dx) / x, 0.0)
+        dw = np.where(self.box, (self.rmw + w * dx) / self.s, 0.0)
+        self.sets[3 if corrector else 2] = [dx, dy, dz, dw]
+        return all(np.isfinite(v).all() for v in (dx, dy, dz, dw)), accepted, its, rel
+
     # -- device-resident IPM vectors (psipm_ipm_*), in NumPy -----------------
     def ipm_load(self, c, b, u, pos, box):
         self.c, self.b, self.u = (np.array(v, dtype=float) for v in (c, b, u))

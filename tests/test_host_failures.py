@@ -10,6 +10,7 @@ exception from ``factorize`` and a ``KKTSolveError`` from ``solve`` make
 import numpy as np
 import pytest
 
+from _helpers import exact_direction
 from fake_device import FakeDevice
 from psipm_b200 import _lib, ipm, synthetic
 from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner, KKTSolveError
@@ -17,8 +18,8 @@ from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner, KKTSolveError
 OPTS = dict(full_preconditioner_row_threshold=10)
 
 
-def make(lp, dev):
-    return GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev, **OPTS)
+def make(lp, dev, **kw):
+    return GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev, **OPTS, **kw)
 
 
 @pytest.fixture(scope="module")
@@ -60,7 +61,7 @@ def test_cuda_error_in_solve_becomes_kkt_error(lp):
 
 def test_breakdown_triggers_retry_with_growth_then_error(lp):
     dev = FakeDevice(lp.A)
-    solver = make(lp, dev)
+    solver = make(lp, dev, minres_fallback=False)
     solver.factorize(np.ones(lp.A.shape[1]), 1.0)
     target = solver.core_target
     dev.fail["solve_info"] = [-2, -2]  # breakdown on the first try and on the retry
@@ -69,6 +70,32 @@ def test_breakdown_triggers_retry_with_growth_then_error(lp):
     assert solver.pcg_retries == 1
     assert solver.core_target > target or solver.core_target == solver.max_core_target
     assert solver.krylov_breakdowns == 1
+
+
+def test_breakdown_after_retry_falls_back_to_minres(lp):
+    """PCG breaks down on the first try and on the retry: the solver answers
+    with the augmented MINRES (psipm_spectral_preconditioner.py:717-737)."""
+    dev = FakeDevice(lp.A)
+    solver = make(lp, dev)
+    solver.factorize(np.ones(lp.A.shape[1]), 1.0)
+    dev.fail["solve_info"] = [-2, -2]
+    r1 = np.random.default_rng(1).standard_normal(lp.A.shape[1])
+    dx, dy = solver.solve(r1, lp.b)
+    assert solver.minres_fallbacks == 1 and solver.full_fallbacks == 1
+    assert solver.minres_iterations > 0 and solver.cg_failures == 1
+    ex_dx, ex_dy = exact_direction(lp.A, solver.theta, solver.delta, r1, lp.b)
+    assert np.linalg.norm(dy - ex_dy) <= 1e-4 * np.linalg.norm(ex_dy)
+
+
+def test_minres_failure_is_a_kkt_error(lp):
+    dev = FakeDevice(lp.A)
+    solver = make(lp, dev)
+    solver.factorize(np.ones(lp.A.shape[1]), 1.0)
+    dev.fail["solve_info"] = [-2, -2]
+    dev.fail["minres"] = [_lib.ERR_CUDA]
+    with pytest.raises(KKTSolveError):
+        solver.solve(np.zeros(lp.A.shape[1]), lp.b)
+    assert solver.minres_fallbacks == 1
 
 
 def test_device_deadline_code_is_reported(lp):
