@@ -93,6 +93,18 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr,
 void psipm_destroy(psipm_handle* h);
 const char* psipm_last_error(const psipm_handle* h);
 
+/* ---- F3 extracted dense columns ----------------------------------------------
+ * Declare the (sorted) columns that the factor leaves out and corrects by
+ * Woodbury, as low_rank_normal_columns chose them (psipm_active_pool.py:691-718,
+ * at most PSIPM_LOW_RANK_MAX): they leave the candidate set and the assembled
+ * diagonal (A_factor), the scores' diagonal adds A2_low_rank w_L
+ * (psipm_stable_preconditioner.py:298-303), and every successful psipm_factor
+ * prepares B = P_base^{-1} A_L and the Cholesky factor of
+ * Theta_L + A_L^T B (psipm_active_pool.py:906-947), which every apply then
+ * uses (:949-956).  Call once, before any core and before set_theta; FP64 only. */
+#define PSIPM_LOW_RANK_MAX 8
+int psipm_set_low_rank(psipm_handle* h, const int64_t* cols, int64_t q);
+
 /* Number and (global, ascending) indices of the candidate columns: columns
  * with at least two nonzeros (psipm_stable_preconditioner.py:169-172). */
 int64_t psipm_num_candidates(const psipm_handle* h);

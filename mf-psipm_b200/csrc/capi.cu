@@ -159,6 +159,16 @@ struct psipm_handle {
     IpmStore ipm;
     MinresWork minres;
 
+    // F3: extracted dense columns and their Woodbury correction
+    std::vector<int64_t> lr_cols;
+    std::vector<int> lr_ptr_host, lr_row_host;
+    std::vector<double> lr_val_host;
+    DevBuf<unsigned char> lr_mask;          // n: 1 on the extracted columns
+    DevBuf<int> lr_ptr, lr_row;             // their CSC slices (q + 1, nnz)
+    DevBuf<double> lr_val, lr_B, lr_chol;   // values; B = P_base^{-1} A_L (m x q); core Cholesky (q x q)
+    DevBuf<double> d_lr, diag_score, lr_part;
+    bool lr_ready = false;
+
     // selection scratch
     DevBuf<unsigned char> flag_a, flag_b, flag_c, mand_flags;
     DevBuf<int> eq, eqscan;
@@ -371,6 +381,15 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
         pc.fvec = fs.fvec.p;
         pc.GT = fs.GT.p;
         pc.gt_off = h->s_panel_off.p;
+        if (h->lr_ready) {
+            pc.lr_q = (int)h->lr_cols.size();
+            pc.lr_ptr = h->lr_ptr.p;
+            pc.lr_row = h->lr_row.p;
+            pc.lr_val = h->lr_val.p;
+            pc.lr_B = h->lr_B.p;
+            pc.lr_chol = h->lr_chol.p;
+            pc.lr_part = h->lr_part.p;
+        }
     }
     PcgStore<T>& st = pstore(h, tag);
     const int64_t m = h->m, n = h->n;
@@ -607,8 +626,23 @@ void compute_weights(psipm_handle* h) {
     h->w.reserve(n);
     h->diag_full.reserve(m);
     LAUNCH(h, k_weights<<<blocks_for(n, 256), 256, 0, h->stream>>>(n, h->theta.p, h->w.p));
+    const bool lr = !h->lr_cols.empty();
     LAUNCH(h, k_diag_full<<<blocks_for(m, 256), 256, 0, h->stream>>>(
-                  (int)m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->w.p, h->diag_full.p));
+                  (int)m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->w.p, lr ? h->lr_mask.p : nullptr,
+                  h->diag_full.p));
+    if (lr) {
+        // scores see A2_factor w_F + A2_low_rank w_L (psipm_stable_preconditioner.py:298-303)
+        h->d_lr.zero(m, h->stream);
+        h->diag_score.reserve(m);
+        for (size_t a = 0; a < h->lr_cols.size(); ++a) {
+            const int nnz = h->lr_ptr_host[a + 1] - h->lr_ptr_host[a];
+            LAUNCH(h, k_diag_lr_column<<<blocks_for(nnz, 256), 256, 0, h->stream>>>(
+                          nnz, h->lr_row.p + h->lr_ptr_host[a], h->lr_val.p + h->lr_ptr_host[a], h->w.p,
+                          (long long)h->lr_cols[a], h->d_lr.p));
+        }
+        LAUNCH(h, k_add_rn<<<blocks_for(m, 256), 256, 0, h->stream>>>((int)m, h->diag_full.p, h->d_lr.p,
+                                                                      h->diag_score.p));
+    }
     if (h->precision == PSIPM_FP32_REFINED) {
         h->wf.reserve(n);
         LAUNCH(h, k_cast<float><<<blocks_for(n, 256), 256, 0, h->stream>>>(n, h->w.p, h->wf.p));
@@ -870,6 +904,83 @@ void copy_out(psipm_handle* h, double* host, const double* dev, int64_t n) {
     if (host && n) PSIPM_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
 }
 
+__global__ void k_scatter_column(int nnz, const int* __restrict__ rows, const double* __restrict__ vals,
+                                 double* __restrict__ dense) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nnz) dense[rows[e]] = vals[e];
+}
+
+// F3: after a numeric factorisation, the Woodbury data for the extracted dense
+// columns (psipm_active_pool.py:906-947): B = P_base^{-1} A_L by q applies of
+// the base factor, the core C = A_L^T B + Theta_L (symmetrised) and its
+// Cholesky factor with the relative shift ladder (0, 1e-14, ..., 1e-8).
+void prepare_low_rank(psipm_handle* h) {
+    require(h->precision == PSIPM_FP64, PSIPM_ERR_UNSUPPORTED, "dense-column extraction is FP64 only");
+    const int q = (int)h->lr_cols.size();
+    const int64_t m = h->m;
+    cudaStream_t st = h->stream;
+    h->lr_B.reserve((int64_t)q * m);
+    DevBuf<double> dense;
+    dense.reserve(m);
+    PcgArgs<double, double> a = pcg_args<double, double>(h);  // lr_ready is false: the base apply
+    for (int c = 0; c < q; ++c) {
+        const int nnz = h->lr_ptr_host[c + 1] - h->lr_ptr_host[c];
+        PSIPM_CUDA(cudaMemsetAsync(dense.p, 0, m * sizeof(double), st));
+        LAUNCH(h, k_scatter_column<<<blocks_for(nnz, 256), 256, 0, st>>>(nnz, h->lr_row.p + h->lr_ptr_host[c],
+                                                                         h->lr_val.p + h->lr_ptr_host[c], dense.p));
+        const double* in = dense.p;
+        double* out = h->lr_B.p + (int64_t)c * m;
+        void* args[] = {&a, (void*)&in, (void*)&out};
+        launch_coop(h, (const void*)k_apply<double, double>, args);
+    }
+    std::vector<double> B((size_t)q * m), th(q);
+    PSIPM_CUDA(cudaMemcpyAsync(B.data(), h->lr_B.p, B.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    for (int c = 0; c < q; ++c)
+        PSIPM_CUDA(cudaMemcpyAsync(&th[c], h->theta.p + h->lr_cols[c], sizeof(double), cudaMemcpyDeviceToHost, st));
+    PSIPM_CUDA(cudaStreamSynchronize(st));
+    std::vector<double> core((size_t)q * q, 0.0);
+    for (int c = 0; c < q; ++c)
+        for (int d = 0; d < q; ++d) {
+            double acc = 0.0;
+            for (int e = h->lr_ptr_host[c]; e < h->lr_ptr_host[c + 1]; ++e)
+                acc += h->lr_val_host[e] * B[(size_t)d * m + h->lr_row_host[e]];
+            core[(size_t)c * q + d] = acc;
+        }
+    for (int c = 0; c < q; ++c) core[(size_t)c * q + c] += th[c];
+    for (int c = 0; c < q; ++c)
+        for (int d = 0; d < c; ++d) {
+            const double v = 0.5 * (core[(size_t)c * q + d] + core[(size_t)d * q + c]);
+            core[(size_t)c * q + d] = core[(size_t)d * q + c] = v;
+        }
+    double scale = 1.0;
+    for (int c = 0; c < q; ++c) scale = std::max(scale, std::fabs(core[(size_t)c * q + c]));
+    for (double rel : {0.0, 1e-14, 1e-12, 1e-10, 1e-8}) {
+        std::vector<double> L((size_t)q * q, 0.0);
+        bool ok = true;
+        for (int i = 0; i < q && ok; ++i)
+            for (int j = 0; j <= i; ++j) {
+                double v = core[(size_t)i * q + j] + (i == j ? rel * scale : 0.0);
+                for (int k = 0; k < j; ++k) v -= L[(size_t)i * q + k] * L[(size_t)j * q + k];
+                if (i == j) {
+                    if (!(v > 0.0)) {
+                        ok = false;
+                        break;
+                    }
+                    L[(size_t)i * q + i] = std::sqrt(v);
+                } else {
+                    L[(size_t)i * q + j] = v / L[(size_t)j * q + j];
+                }
+            }
+        if (!ok) continue;
+        h->lr_chol.upload(L, st);
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        h->lr_ready = true;
+        return;
+    }
+    h->have_factor = false;
+    throw Failure(PSIPM_ERR_NOT_PD, "low-rank correction is not positive definite");
+}
+
 }  // namespace
 
 namespace {
@@ -988,6 +1099,47 @@ void psipm_destroy(psipm_handle* h) {
 
 const char* psipm_last_error(const psipm_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
+int psipm_set_low_rank(psipm_handle* h, const int64_t* cols, int64_t q) {
+    if (q < 0 || q > PSIPM_LOW_RANK_MAX || (q && !cols)) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        if ((int64_t)h->lr_cols.size() == q && std::equal(h->lr_cols.begin(), h->lr_cols.end(), cols)) return;
+        require(!h->have_symbolic && h->core.empty(), PSIPM_ERR_STATE, "set_low_rank after a core was set");
+        require(q == 0 || h->precision == PSIPM_FP64, PSIPM_ERR_UNSUPPORTED, "dense-column extraction is FP64 only");
+        for (int64_t t = 0; t < q; ++t)
+            require(cols[t] >= 0 && cols[t] < h->n && (t == 0 || cols[t] > cols[t - 1]), PSIPM_ERR_ARGUMENT,
+                    "low-rank columns must be sorted, distinct and in range");
+        const int64_t n = h->n;
+        cudaStream_t st = h->stream;
+        h->lr_cols.assign(cols, cols + q);
+        std::vector<unsigned char> mask(std::max<int64_t>(1, n), 0);
+        h->lr_ptr_host.assign(1, 0);
+        h->lr_row_host.clear();
+        h->lr_val_host.clear();
+        for (int64_t t = 0; t < q; ++t) {
+            const int64_t j = cols[t];
+            mask[j] = 1;
+            for (int64_t e = h->colptr[j]; e < h->colptr[j + 1]; ++e) {
+                h->lr_row_host.push_back(h->rowidx[e]);
+                h->lr_val_host.push_back(h->val[e]);
+            }
+            h->lr_ptr_host.push_back((int)h->lr_row_host.size());
+        }
+        h->lr_mask.upload(mask, st);
+        h->lr_ptr.upload(h->lr_ptr_host, st);
+        h->lr_row.upload(h->lr_row_host.empty() ? std::vector<int>(1, 0) : h->lr_row_host, st);
+        h->lr_val.upload(h->lr_val_host.empty() ? std::vector<double>(1, 0.0) : h->lr_val_host, st);
+        h->lr_part.reserve((int64_t)std::max(1, h->coop_blocks) * kLowRankMax);
+        h->lr_ready = false;
+        // the candidates of the factor exclude the extracted columns (psipm_stable_preconditioner.py:169-172)
+        h->cand.clear();
+        for (int64_t j = 0; j < n; ++j)
+            if (!mask[j] && h->colptr[j + 1] - h->colptr[j] >= 2) h->cand.push_back(j);
+        std::vector<long long> cl(h->cand.begin(), h->cand.end());
+        h->d_cand.upload(cl, st);
+        h->have_theta = false;
+    });
+}
+
 int64_t psipm_num_candidates(const psipm_handle* h) { return h ? (int64_t)h->cand.size() : -1; }
 
 int psipm_get_candidates(const psipm_handle* h, int64_t* out) {
@@ -1014,7 +1166,8 @@ int psipm_scores(psipm_handle* h, double fill_weight, double* scores, double* di
         const double tiny = 2.2250738585072014e-308;
         h->inv.reserve(m);
         h->scores.reserve(std::max<int64_t>(1, nc));
-        LAUNCH(h, k_inv_diag<<<blocks_for(m, 256), 256, 0, h->stream>>>((int)m, h->diag_full.p,
+        const double* diag = h->lr_cols.empty() ? h->diag_full.p : h->diag_score.p;
+        LAUNCH(h, k_inv_diag<<<blocks_for(m, 256), 256, 0, h->stream>>>((int)m, diag,
                                                                         std::max(h->delta, tiny), h->inv.p));
         if (nc)
             LAUNCH(h, k_scores<<<blocks_for(nc, 256), 256, 0, h->stream>>>(
@@ -1022,7 +1175,7 @@ int psipm_scores(psipm_handle* h, double fill_weight, double* scores, double* di
                           fill_weight, h->scores.p));
         h->scores_valid = true;
         copy_out(h, scores, h->scores.p, nc);
-        copy_out(h, diagonal, h->diag_full.p, m);
+        copy_out(h, diagonal, diag, m);
     });
 }
 
@@ -1165,6 +1318,8 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
         }
         PSIPM_CUDA(cudaStreamSynchronize(st));
         h->have_factor = true;
+        h->lr_ready = false;
+        if (!h->lr_cols.empty()) prepare_low_rank(h);
     });
     return status;
 }

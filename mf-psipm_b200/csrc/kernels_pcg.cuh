@@ -130,6 +130,14 @@ struct PrecLayout {
     int trace_cap = 0;
     T* xp = nullptr;
     T* yp = nullptr;
+    // extracted dense columns: the Woodbury correction of the apply (lr_q = 0: none)
+    int lr_q = 0;
+    const int* lr_ptr = nullptr;      // q + 1 offsets into lr_row / lr_val
+    const int* lr_row = nullptr;
+    const double* lr_val = nullptr;
+    const double* lr_B = nullptr;     // P_base^{-1} A_L, m x q column-major
+    const double* lr_chol = nullptr;  // Cholesky factor of the q x q core, row-major lower
+    double* lr_part = nullptr;        // per-block partial sums, gridDim.x x kLowRankMax
 };
 
 template <typename T, typename P = T>
@@ -473,6 +481,58 @@ __device__ void prec_backward_small(const PrecLayout<P>& pc, int s, P* fs) {
     __syncwarp();
 }
 
+constexpr int kLowRankMax = 8;
+
+// Woodbury correction for the extracted dense columns A_L
+// (psipm_active_pool.py:949-956): with z0 = P_base^{-1} r already in out,
+//   z = z0 - B C^{-1} (A_L^T z0),  B = P_base^{-1} A_L,  C = Theta_L + A_L^T B.
+// The q dot products go through per-block partials that every block sums in
+// the same order, so all blocks hold the same coefficients.
+template <typename P, typename IT>
+__device__ void prec_low_rank(const PrecLayout<P>& pc, const IT* in, IT* out, double& acc_rz,
+                              const GridBarrier& grid) {
+    __shared__ double scr[32];
+    __shared__ double coef[2 * kLowRankMax];
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gstride = gridDim.x * blockDim.x;
+    const int q = pc.lr_q;
+    grid.sync();  // z0 complete
+    for (int a = 0; a < q; ++a) {
+        double t = 0.0;
+        for (int e = pc.lr_ptr[a] + gtid; e < pc.lr_ptr[a + 1]; e += gstride)
+            t += pc.lr_val[e] * (double)__ldcg(out + pc.lr_row[e]);
+        t = block_sum(t, scr);
+        if (threadIdx.x == 0) pc.lr_part[blockIdx.x * kLowRankMax + a] = t;
+    }
+    grid.sync();
+    if (threadIdx.x < q) {
+        double t = 0.0;
+        for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(pc.lr_part + b * kLowRankMax + threadIdx.x);
+        coef[threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // c = L^{-T} L^{-1} t
+        double* c = coef + kLowRankMax;
+        for (int i = 0; i < q; ++i) {
+            double v = coef[i];
+            for (int j = 0; j < i; ++j) v -= pc.lr_chol[i * q + j] * c[j];
+            c[i] = v / pc.lr_chol[i * q + i];
+        }
+        for (int i = q - 1; i >= 0; --i) {
+            double v = c[i];
+            for (int j = i + 1; j < q; ++j) v -= pc.lr_chol[j * q + i] * c[j];
+            c[i] = v / pc.lr_chol[i * q + i];
+        }
+    }
+    __syncthreads();
+    for (int i = gtid; i < pc.m; i += gstride) {
+        double z = (double)out[i];
+        for (int a = 0; a < q; ++a) z -= pc.lr_B[(long long)a * pc.m + i] * coef[kLowRankMax + a];
+        out[i] = (IT)z;
+        acc_rz += (double)in[i] * z;
+    }
+}
+
 // z = P^{-1} in; acc_rz += in . z.  Ends without a barrier (the caller's
 // reduction provides it).
 template <typename P, typename IT>
@@ -525,12 +585,14 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
         grid.sync();
         mark();
     }
+    const bool lr = pc.lr_q > 0;
     for (int i = gtid; i < pc.m; i += gstride) {
         const int k = pc.iperm[i];
         const IT zi = (IT)(pc.dscp[k] * pc.yp[k]);
         out[i] = zi;
-        acc_rz += (double)in[i] * (double)zi;
+        if (!lr) acc_rz += (double)in[i] * (double)zi;
     }
+    if (lr) prec_low_rank(pc, in, out, acc_rz, grid);
 }
 
 // H v into phase-B epilogue `mode` (A, barrier, B [, barrier, B2]); ends after

@@ -23,18 +23,37 @@ __global__ void k_weights(long long n, const double* __restrict__ theta, double*
     if (j < n) w[j] = __ddiv_rn(1.0, theta[j]);
 }
 
-// diag_full_i = sum_j (a_ij^2) w_j over row i in column order (A2_factor @ w)
+// diag_full_i = sum_j (a_ij^2) w_j over row i in column order (A2_factor @ w);
+// columns with skip[j] != 0 (extracted dense columns) are left out
 __global__ void k_diag_full(int m, const int* __restrict__ a_ptr, const int* __restrict__ a_idx,
                             const double* __restrict__ a_val, const double* __restrict__ w,
-                            double* __restrict__ diag) {
+                            const unsigned char* __restrict__ skip, double* __restrict__ diag) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     double acc = 0.0;
     for (int k = a_ptr[i]; k < a_ptr[i + 1]; ++k) {
+        const int j = a_idx[k];
+        if (skip && skip[j]) continue;
         const double a = a_val[k];
-        acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(a, a), w[a_idx[k]]));
+        acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(a, a), w[j]));
     }
     diag[i] = acc;
+}
+
+// d_i += a_ij^2 w_j over one extracted column j (A2_low_rank @ w_L, one launch
+// per column in ascending column order, as the sparse product sums them)
+__global__ void k_diag_lr_column(int nnz, const int* __restrict__ rows, const double* __restrict__ vals,
+                                 const double* __restrict__ w, long long j, double* __restrict__ d) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const double a = vals[e];
+    d[rows[e]] = __dadd_rn(d[rows[e]], __dmul_rn(__dmul_rn(a, a), w[j]));
+}
+
+__global__ void k_add_rn(int m, const double* __restrict__ a, const double* __restrict__ b,
+                         double* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = __dadd_rn(a[i], b[i]);
 }
 
 // inv_i = 1 / max(diag_i + max(delta, tiny), tiny)

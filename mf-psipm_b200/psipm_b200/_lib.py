@@ -93,6 +93,7 @@ SIGNATURES = {
     "psipm_create": (_I32, [_I64, _I64, _I64, _P, _P, _P, _I32, _I32, ctypes.POINTER(_P)]),
     "psipm_destroy": (None, [_P]),
     "psipm_last_error": (ctypes.c_char_p, [_P]),
+    "psipm_set_low_rank": (_I32, [_P, _P, _I64]),
     "psipm_num_candidates": (_I64, [_P]),
     "psipm_get_candidates": (_I32, [_P, _P]),
     "psipm_set_theta": (_I32, [_P, _P, _D]),

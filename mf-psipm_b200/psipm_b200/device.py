@@ -103,6 +103,14 @@ class NormalEquationsDevice:
         return float(out.value)
 
     # -- operations -----------------------------------------------------------
+    def set_low_rank(self, columns: np.ndarray) -> None:
+        """Extracted dense columns (psipm_set_low_rank); the candidates change."""
+        cols = i64(np.sort(np.asarray(columns)))
+        self._check(self.lib.psipm_set_low_rank(self.h, ptr(cols), cols.size))
+        ncand = self.lib.psipm_num_candidates(self.h)
+        self.candidates = np.empty(ncand, dtype=np.int64)
+        self._check(self.lib.psipm_get_candidates(self.h, ptr(self.candidates)))
+
     def set_theta(self, theta: np.ndarray, delta: float) -> None:
         theta = f64(theta)
         if theta.shape != (self.n,):

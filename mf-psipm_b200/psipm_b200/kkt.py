@@ -150,10 +150,8 @@ class GpuStableActiveColumnPreconditioner:
         self.low_rank_columns = (low_rank_normal_columns(A, int(low_rank_max_columns), int(low_rank_min_nnz),
                                                          float(low_rank_clique_ratio))
                                  if extract_low_rank else np.empty(0, dtype=np.int64))
-        if self.low_rank_columns.size:
-            raise NotImplementedError(
-                "Woodbury-extracted dense columns (psipm_active_pool.py:906-956) are not supported "
-                "by the device factor yet")
+        if self.low_rank_columns.size and precision != _lib.FP64:
+            raise NotImplementedError("Woodbury-extracted dense columns need the FP64 device factor")
         # an existing device handle for the same A may be reused (its matrix
         # upload is skipped); its core is cleared so the policy starts afresh
         self.dev = dev if dev is not None else NormalEquationsDevice(A, device=device, precision=precision)
@@ -162,13 +160,18 @@ class GpuStableActiveColumnPreconditioner:
                 raise ValueError("the device handle holds a different matrix")
             dev.set_core(np.empty(0, dtype=np.int64))
         self.precision = precision
-        self.factor_columns = np.arange(self.n, dtype=np.int64)
+        if self.low_rank_columns.size:
+            # the factor leaves these columns out and corrects for them by
+            # Woodbury (psipm_active_pool.py:786-798, 906-956)
+            self.dev.set_low_rank(self.low_rank_columns)
+        self.factor_columns = np.setdiff1d(np.arange(self.n, dtype=np.int64), self.low_rank_columns)
         self.candidates = self.dev.candidates
         counts = np.diff(A.indptr)[self.candidates].astype(float)
         self.clique_burden = 0.5 * counts * np.maximum(counts - 1.0, 0.0)
+        factor_nnz = A.nnz - int(np.diff(A.indptr)[self.low_rank_columns].sum())
         self.use_full_preconditioner = bool(
             self.m <= max(0, int(full_preconditioner_row_threshold))
-            and A.nnz <= max(0, int(full_preconditioner_nnz_limit))
+            and factor_nnz <= max(0, int(full_preconditioner_nnz_limit))
             and float(self.clique_burden.sum()) <= float(full_preconditioner_clique_limit)
         )
         prot = np.zeros(self.n, dtype=bool)

@@ -96,6 +96,31 @@ def random_lp(m: int = 2000, n: int = 6000, per_column: int = 5, seed: int = 0) 
                    dict(family="random_lp", m=m, n=n, seed=seed))
 
 
+def random_lp_dense(m: int = 1200, n: int = 3600, dense: int = 4, dense_nnz: int = 1100, per_column: int = 5,
+                    seed: int = 0) -> StandardLP:
+    """``random_lp`` whose first ``dense`` columns hold ``dense_nnz`` entries each.
+
+    Such columns (>= 1,024 entries, large potential clique in A A^T) are the
+    ones the reference leaves out of the factor and corrects for by Woodbury
+    (psipm_active_pool.py:691-718, 906-956); the other families have none.
+    """
+    rng = np.random.default_rng(seed)
+    base = random_lp(m, n, per_column, seed)
+    A = base.A.tolil()
+    for j in range(min(dense, n)):
+        rows = rng.choice(m, min(dense_nnz, m), replace=False)
+        A[:, j] = 0.0
+        A[rows, j] = rng.standard_normal(rows.size)[:, None]
+    A = sp.csc_matrix(A)
+    x0 = rng.uniform(0.5, 1.5, n)
+    b = A @ x0
+    y0 = rng.standard_normal(m)
+    s0 = rng.uniform(0.1, 1.0, n)
+    c = A.T @ y0 + s0
+    return _finish(A, b, c, np.full(n, np.inf), f"random_lp_dense_m{m}_n{n}_d{dense}_s{seed}",
+                   dict(family="random_lp_dense", m=m, n=n, dense=dense, dense_nnz=dense_nnz, seed=seed))
+
+
 def _ground(A: sp.csc_matrix) -> np.ndarray:
     """Rows to keep after removing one row per connected component.
 

@@ -36,6 +36,8 @@ INSTANCES = {
     "random_m300": ("random_lp", dict(m=300, n=900, seed=0)),
     "grid_20x25": ("grid_network", dict(rows=20, cols=25, seed=1000)),
     "cover_m200": ("set_cover", dict(m=200, n=10_000, seed=2000)),
+    # four dense columns (1,100 entries each): the Woodbury extraction path
+    "dense_m1200": ("random_lp_dense", dict(m=1200, n=3600, seed=7)),
 }
 # plus hsd_m1600 (make_hsd): the V3.1 HSD preconditioner surface
 # the small instances use the stable core path (the exact-preconditioner
@@ -108,6 +110,7 @@ def main():
             pcg_iterations=sol.pcg_iterations, cg_iterations=np.array(solver.cg_iterations),
             core_sizes=np.array(solver.core_sizes), n_fact=solver.n_fact,
             candidates=solver.candidates, matching_columns=solver.matching_columns,
+            low_rank_columns=np.asarray(solver.low_rank_columns, dtype=np.int64),
             n_factor_calls=len(solver.rec_factor), n_solve_calls=len(solver.rec_solve),
             n_cores=len(solver.rec_cores),
         )
