@@ -94,7 +94,8 @@ struct psipm_handle {
     // device matrix
     DevBuf<int> at_ptr, at_idx, a_ptr, a_idx;
     DevBuf<double> at_val, a_val;
-    DevBuf<int> short_rows, long_rows, long_chunk_ptr, chunk_beg, chunk_end;
+    DevBuf<int> short_rows, long_rows, long_chunk_ptr, chunk_beg, chunk_end, chunk_row;
+    int64_t short_nnz = 0;
     int n_short = 0, n_long = 0, n_chunks = 0, vw = 32;
     DevBuf<long long> d_cand;
 
@@ -256,7 +257,7 @@ void build_matrix(psipm_handle* h) {
         PSIPM_CUDA(cudaStreamSynchronize(h->stream));
     }
     // short / long rows
-    std::vector<int> shortr, longr, lcp{0}, cb, ce;
+    std::vector<int> shortr, longr, lcp{0}, cb, ce, crow;
     int64_t short_nnz = 0, short_cnt = 0;
     for (int64_t i = 0; i < m; ++i) {
         int len = a_ptr[i + 1] - a_ptr[i];
@@ -265,6 +266,7 @@ void build_matrix(psipm_handle* h) {
             for (int b = a_ptr[i]; b < a_ptr[i + 1]; b += kLongRow) {
                 cb.push_back(b);
                 ce.push_back(std::min(b + kLongRow, a_ptr[i + 1]));
+                crow.push_back((int)i);
             }
             lcp.push_back((int)cb.size());
         } else {
@@ -285,6 +287,8 @@ void build_matrix(psipm_handle* h) {
     h->long_chunk_ptr.upload(lcp, h->stream);
     h->chunk_beg.upload(cb, h->stream);
     h->chunk_end.upload(ce, h->stream);
+    h->chunk_row.upload(crow, h->stream);
+    h->short_nnz = short_nnz;
     // candidates: columns with at least two nonzeros
     h->cand.clear();
     for (int64_t j = 0; j < n; ++j)
@@ -1382,21 +1386,86 @@ int psipm_pcg(psipm_handle* h, const double* rhs, double tol, int32_t maxit, int
 // ---- H1 solve --------------------------------------------------------------
 namespace {
 
+// y[rows[r]] = (row rows[r] of CSR M) . v, W lanes per listed row
+template <int W>
+__global__ void k_list_rows(int nrows, const int* __restrict__ rows, const int* __restrict__ ptr,
+                            const int* __restrict__ idx, const double* __restrict__ val,
+                            const double* __restrict__ v, double* __restrict__ y) {
+    constexpr int kRowsPerWarp = 32 / W;
+    const int lane = threadIdx.x & (W - 1);
+    const int sub = (threadIdx.x & 31) / W;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * kRowsPerWarp; base < nrows; base += nwarps * kRowsPerWarp) {
+        const long long r = base + sub;
+        const int i = r < nrows ? rows[r] : 0;
+        double acc = 0.0;
+        if (r < nrows)
+            for (int k = ptr[i] + lane; k < ptr[i + 1]; k += W) acc += val[k] * v[idx[k]];
+#pragma unroll
+        for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, W);
+        if (lane == 0 && r < nrows) y[i] = acc;
+    }
+}
+
+// long rows: one warp per 4,096-entry chunk, partial sums added with atomics
+// into the zeroed outputs of those rows
+__global__ void k_chunk_rows(int nchunks, const int* __restrict__ cbeg, const int* __restrict__ cend,
+                             const int* __restrict__ crow, const int* __restrict__ idx,
+                             const double* __restrict__ val, const double* __restrict__ v,
+                             double* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long c = warp; c < nchunks; c += nwarps) {
+        double acc = 0.0;
+        for (int k = cbeg[c] + lane; k < cend[c]; k += 32) acc += val[k] * v[idx[k]];
+        acc = warp_sum(acc);
+        if (lane == 0) atomicAdd(&y[crow[c]], acc);
+    }
+}
+
+__global__ void k_zero_rows(int nrows, const int* __restrict__ rows, double* __restrict__ y) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrows) y[rows[r]] = 0.0;
+}
+
+// y = A v (m rows, FP64) for any row lengths: the short rows by sub-warps
+// sized to their mean length, the long rows in chunks.  Long-row sums are
+// combined with atomics, so y is reproducible to rounding.
+void a_times(psipm_handle* h, const double* v, double* y) {
+    cudaStream_t st = h->stream;
+    const int ns = h->n_short;
+    if (ns) {
+        const double mean = (double)h->short_nnz / ns;
+        const int grid = (int)std::min<int64_t>(std::max<int64_t>(1, ns / 8), (int64_t)h->num_sms * 16);
+        if (mean <= 3.0)
+            LAUNCH(h, k_list_rows<1><<<grid, 256, 0, st>>>(ns, h->short_rows.p, h->a_ptr.p, h->a_idx.p, h->a_val.p, v, y));
+        else if (mean <= 12.0)
+            LAUNCH(h, k_list_rows<4><<<grid, 256, 0, st>>>(ns, h->short_rows.p, h->a_ptr.p, h->a_idx.p, h->a_val.p, v, y));
+        else if (mean <= 48.0)
+            LAUNCH(h, k_list_rows<8><<<grid, 256, 0, st>>>(ns, h->short_rows.p, h->a_ptr.p, h->a_idx.p, h->a_val.p, v, y));
+        else
+            LAUNCH(h, k_list_rows<32><<<grid, 256, 0, st>>>(ns, h->short_rows.p, h->a_ptr.p, h->a_idx.p, h->a_val.p, v, y));
+    }
+    if (h->n_long) {
+        LAUNCH(h, k_zero_rows<<<blocks_for(h->n_long, 256), 256, 0, st>>>(h->n_long, h->long_rows.p, y));
+        const int grid = (int)std::min<int64_t>(blocks_for((int64_t)h->n_chunks * 32, 256), (int64_t)h->num_sms * 16);
+        LAUNCH(h, k_chunk_rows<<<grid, 256, 0, st>>>(h->n_chunks, h->chunk_beg.p, h->chunk_end.p, h->chunk_row.p,
+                                                     h->a_idx.p, h->a_val.p, v, y));
+    }
+}
+
+__global__ void k_sub(long long n, const double* __restrict__ b, const double* __restrict__ a,
+                      double* __restrict__ out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = b[i] - a[i];
+}
+
 __global__ void k_div(long long n, const double* __restrict__ a, const double* __restrict__ b,
                       double* __restrict__ out) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) out[i] = a[i] / b[i];
-}
-
-// out_i = b_i - sum_j A_ij v_j   (A in CSR)
-__global__ void k_rhs(int m, const int* __restrict__ ptr, const int* __restrict__ idx,
-                      const double* __restrict__ val, const double* __restrict__ v,
-                      const double* __restrict__ b, double* __restrict__ out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    double s = 0.0;
-    for (int k = ptr[i]; k < ptr[i + 1]; ++k) s += val[k] * v[idx[k]];
-    out[i] = b[i] - s;
 }
 
 // dx_j = wr1_j + (sum_i A_ij dy_i) / theta_j
@@ -1575,8 +1644,9 @@ void solve_device(psipm_handle* h, const double* r1d, const double* r2d, double 
     h->wr1.reserve(n);
     h->rhs64.reserve(m);
     LAUNCH(h, k_div<<<blocks_for(n, 256), 256, 0, st>>>(n, r1d, h->theta.p, h->wr1.p));
-    LAUNCH(h, k_rhs<<<blocks_for(m, 256), 256, 0, st>>>((int)m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->wr1.p,
-                                                         r2d, h->rhs64.p));
+    // rhs = r2 - A (r1 / theta)
+    a_times(h, h->wr1.p, h->rhs64.p);
+    LAUNCH(h, k_sub<<<blocks_for(m, 256), 256, 0, st>>>(m, r2d, h->rhs64.p, h->rhs64.p));
     const double* dy = solve_normal(h, h->rhs64.p, tol, maxit, variant, replacement, gap_tol, info);
     LAUNCH(h, k_dx<<<blocks_for(n, 256), 256, 0, st>>>(n, h->at_ptr.p, h->at_idx.p, h->at_val.p, dy, h->wr1.p,
                                                         h->theta.p, dxd));
@@ -1766,7 +1836,7 @@ double from_bits(unsigned long long b) {
 void ipm_products(psipm_handle* h) {
     IpmStore& I = h->ipm;
     spmv_csr(h, h->n, h->nnz, h->at_ptr.p, h->at_idx.p, h->at_val.p, I.y.p, I.aty.p);
-    spmv_csr(h, h->m, h->nnz, h->a_ptr.p, h->a_idx.p, h->a_val.p, I.x.p, I.ax.p);
+    a_times(h, I.x.p, I.ax.p);
 }
 
 template <typename U>
@@ -2104,7 +2174,7 @@ struct MinresState {
 
     void aug_matvec(const double* v, double* out) {  // out = K v
         spmv_csr(h, n, h->nnz, h->at_ptr.p, h->at_idx.p, h->at_val.p, v + n, out);
-        spmv_csr(h, m, h->nnz, h->a_ptr.p, h->a_idx.p, h->a_val.p, v, out + n);
+        a_times(h, v, out + n);
         LAUNCH(h, k_aug_finish<<<blocks_for(len, kIpmThreads), kIpmThreads, 0, h->stream>>>(n, m, h->theta.p,
                                                                                                h->delta, v, out));
     }
