@@ -15,7 +15,8 @@ and so plugs into ``psipm_solve(lp, kkt_solver=...)``
 
 :class:`GpuStableColumnPreconditioner` is the V3.1 HSD preconditioner
 surface (psipm_v3_1_hsd.py:823-989) and :func:`pcg_rows` the device
-replacement of its ``_pcg`` (:1015-1063).
+replacement of its ``_pcg`` (:1015-1063); :mod:`psipm_b200.hsd` builds the
+reduced HSD Newton system (:1066-1264) on top of both.
 
 There is no CPU fallback: without the CUDA library every constructor raises
 ``GpuUnavailable``.
@@ -752,6 +753,20 @@ class GpuStableColumnPreconditioner:
     def record_solve(self, iterations, elapsed, converged) -> None:
         self.record_iterations(iterations, elapsed, converged)
 
+    def solve_normal(self, r1, r2, rtol, max_iterations, deadline=np.inf):
+        """``dy = H^{-1} (r2 - A D r1)`` by the HSD PCG (psipm_v3_1_hsd.py:1015-1063)
+        and ``dx = D (r1 + A' dy)``, both on the device; ``D`` are the weights of
+        the last :meth:`factor` call (``1/theta`` with ``theta = 1/max(D, TINY)``).
+
+        One ``psipm_solve`` call: the right-hand side's SpMV, the PCG and the
+        back-substitution run on the device; r1, r2 go in and dx, dy come out.
+        Returns ``(dx, dy, iterations, matvecs, okay, elapsed)``; the deadline
+        limits the launch as in :func:`pcg_rows`.
+        """
+        started = time.perf_counter()
+        dx, res = self.impl.dev.solve(r1, r2, rtol, _deadline_iterations(max_iterations, deadline), _lib.PCG_HSD)
+        return dx, res.x, res.iterations, res.matvecs, bool(res.ok), time.perf_counter() - started
+
 
 def pcg_rows(preconditioner: GpuStableColumnPreconditioner, rhs, rtol, max_iterations, deadline=np.inf):
     """Device replacement of the HSD ``_pcg`` (psipm_v3_1_hsd.py:1015-1063).
@@ -762,7 +777,16 @@ def pcg_rows(preconditioner: GpuStableColumnPreconditioner, rhs, rtol, max_itera
     (psipm_v3_1_hsd.py:1136-1137).
     """
     started = time.perf_counter()
-    res = preconditioner.impl.dev.pcg(rhs, rtol, int(max_iterations), _lib.PCG_HSD)
-    if time.perf_counter() >= deadline and not res.ok:
-        return res.x, res.iterations, res.matvecs, False, time.perf_counter() - started
+    res = preconditioner.impl.dev.pcg(rhs, rtol, _deadline_iterations(max_iterations, deadline), _lib.PCG_HSD)
     return res.x, res.iterations, res.matvecs, bool(res.ok), time.perf_counter() - started
+
+
+def _deadline_iterations(max_iterations, deadline) -> int:
+    """Iteration limit of one device PCG launch under the caller's deadline.
+
+    The reference tests the deadline after each iteration's convergence test
+    (psipm_v3_1_hsd.py:1054-1055), so a call that starts past it stops after
+    one iteration, converged or not.  The device PCG runs as one launch, so
+    the deadline is tested when it starts: one iteration if it has passed.
+    """
+    return 1 if time.perf_counter() >= deadline and max_iterations > 0 else int(max_iterations)

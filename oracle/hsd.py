@@ -4,6 +4,12 @@
   every 10 iterations (psipm_v3_1_hsd.py:1015-1063).
 * :class:`StableColumnPreconditionerOracle` — the V3.1 wrapper around the
   stable active-column preconditioner (psipm_v3_1_hsd.py:823-989).
+* :class:`HSDNewtonSystemOracle` — the reduced HSD Newton system
+  (psipm_v3_1_hsd.py:1066-1264): border data, three normal-equations solves,
+  the 2 x 2 border solve and the back-substitution.
+
+Pinned bit-exact to the reference on the fixtures hsd_m1600 and
+hsd_newton_m1600 (tests/test_hsd_oracle.py).
 """
 
 from __future__ import annotations
@@ -110,3 +116,109 @@ class StableColumnPreconditionerOracle:
                 self.growth_events += 1
             impl.core_age = impl.core_max_age
             self._last_growth_epoch = self._factor_epoch
+
+
+class HSDNewtonSystemOracle:
+    """The reduced HSD Newton system of one active-column set
+    (psipm_v3_1_hsd.py:1066-1264), restated.
+
+    ``state`` supplies x, z, w, tau, kappa; ``embedding`` bar_b, bar_c, bar_g;
+    ``options`` zeta and pcg_max_iterations; ``stats`` the LinearStats counters
+    (iterations, max_iterations, solves, matvecs, failures, seconds,
+    preconditioner_seconds).  The construction factors the preconditioner
+    (:1098) and forms the border data (:1099-1131); ``direction`` solves
+    ``f``, and on its first call also ``h`` and ``theta_row`` (:1160-1264).
+    """
+
+    def __init__(self, A, c, upper, b, D, delta, eta, state, embedding, preconditioner, pcg_tolerance,
+                 options, deadline, stats):
+        self.A, self.c, self.upper, self.b, self.D = A, c, upper, b, D
+        self.delta, self.eta, self.state, self.embedding = delta, eta, state, embedding
+        self.preconditioner, self.pcg_tolerance = preconditioner, pcg_tolerance
+        self.options, self.deadline, self.stats = options, deadline, stats
+        stats.preconditioner_seconds += preconditioner.factor(D, delta)
+        boxed = np.isfinite(upper)
+        self.boxed = boxed
+        slack = np.ones_like(c)
+        slack[boxed] = upper[boxed] * state.tau - state.x[boxed]
+        ratio = np.zeros_like(c)
+        ratio[boxed] = state.w[boxed] / slack[boxed]
+        self.slack, self.upper_ratio = slack, ratio
+        u0 = np.where(boxed, upper, 0.0)
+        self.c_direction = c - ratio * u0
+        self.c_gap = c + ratio * u0
+        bar_b, bar_c = embedding.bar_b, embedding.bar_c
+        self.h = b + A @ (D * self.c_direction)
+        self.g = b - A @ (D * self.c_gap)
+        Dc = A @ (D * bar_c)
+        self.theta_row = bar_b + Dc
+        self.normal_row = Dc - bar_b
+        curvature = float(np.sum(ratio[boxed] * upper[boxed] * upper[boxed]))
+        self.alpha = float(self.c_gap @ (D * self.c_direction)) + curvature + state.kappa / state.tau + eta
+        self.beta = embedding.bar_g - float(self.c_gap @ (D * bar_c))
+        self.gamma = -float(bar_c @ (D * self.c_direction)) - embedding.bar_g
+        self.lambda_theta = float(bar_c @ (D * bar_c)) + options.zeta
+        self._h_solution = None
+        self._theta_solution = None
+
+    def matvec(self, v):  # :1136-1137
+        return self.A @ (self.D * (self.A.T @ v)) + self.delta * v
+
+    def solve_rows(self, rhs):  # :1139-1159
+        x, it, mv, ok, elapsed = pcg(self.matvec, rhs, self.preconditioner, self.pcg_tolerance,
+                                     self.options.pcg_max_iterations, self.deadline)
+        st = self.stats
+        st.solves += 1
+        st.iterations += it
+        st.max_iterations = max(st.max_iterations, it)
+        st.matvecs += mv
+        st.seconds += elapsed
+        if hasattr(self.preconditioner, "record_solve"):
+            self.preconditioner.record_solve(it, elapsed, ok)
+        else:
+            self.preconditioner.record_iterations(it)
+        if not ok:
+            st.failures += 1
+        return x, ok
+
+    def direction(self, rhs_d, rhs_p, rhs_g, rhs_n, rhs_c, rhs_upper, rhs_t):  # :1160-1264
+        st, boxed, D = self.state, self.boxed, self.D
+        up = np.zeros_like(rhs_d)
+        up[boxed] = rhs_upper[boxed] / self.slack[boxed]
+        q = rhs_d + rhs_c / st.x - up
+        u, ok_u = self.solve_rows(-rhs_p - self.A @ (D * q))
+        ok_h = ok_t = True
+        if self._h_solution is None:
+            self._h_solution, ok_h = self.solve_rows(self.h)
+        if self._theta_solution is None:
+            self._theta_solution, ok_t = self.solve_rows(self.theta_row)
+        hs, ts = self._h_solution, self._theta_solution
+        bar_c = self.embedding.bar_c
+        gap_rhs = (rhs_g + float(self.c_gap @ (D * q))
+                   + float(self.upper[boxed] @ (rhs_upper[boxed] / self.slack[boxed]))
+                   + rhs_t / st.tau - float(self.g @ u))
+        normal_rhs = rhs_n - float(bar_c @ (D * q)) - float(self.normal_row @ u)
+        M = np.array([[self.alpha + float(self.g @ hs), self.beta - float(self.g @ ts)],
+                      [self.gamma + float(self.normal_row @ hs), self.lambda_theta - float(self.normal_row @ ts)]],
+                     dtype=np.float64)
+        v = np.array([gap_rhs, normal_rhs], dtype=np.float64)
+        det = float(np.linalg.det(M))
+        scale = max(float(np.linalg.norm(M, ord=np.inf)), 1.0)
+        if not np.all(np.isfinite(M)) or not np.all(np.isfinite(v)) or abs(det) <= 64.0 * EPS * scale * scale:
+            ok_u = False
+            M = M + 64.0 * EPS * scale * np.eye(2)
+        try:
+            dtau, dtheta = np.linalg.solve(M, v)
+        except np.linalg.LinAlgError:
+            dtau, dtheta = np.linalg.lstsq(M, v, rcond=None)[0]
+            ok_u = False
+        dy = u + hs * dtau - ts * dtheta
+        dx = D * (q + self.A.T @ dy - self.c_direction * dtau + bar_c * dtheta)
+        dz = (rhs_c - st.z * dx) / st.x
+        dw = np.zeros_like(dx)
+        ds = np.zeros_like(dx)
+        ds[boxed] = self.upper[boxed] * dtau - dx[boxed]
+        dw[boxed] = (rhs_upper[boxed] - st.w[boxed] * ds[boxed]) / self.slack[boxed]
+        dkappa = (rhs_t - st.kappa * dtau) / st.tau
+        finite = all(np.all(np.isfinite(a)) for a in (dx, dy, dz, dw, np.asarray([dtau, dtheta, dkappa])))
+        return dx, dy, dz, dw, float(dtau), float(dtheta), float(dkappa), bool(ok_u and ok_h and ok_t and finite)

@@ -39,7 +39,8 @@ INSTANCES = {
     # four dense columns (1,100 entries each): the Woodbury extraction path
     "dense_m1200": ("random_lp_dense", dict(m=1200, n=3600, seed=7)),
 }
-# plus hsd_m1600 (make_hsd): the V3.1 HSD preconditioner surface
+# plus hsd_m1600 (make_hsd): the V3.1 HSD preconditioner surface, and
+# hsd_newton_m1600 (make_hsd_newton): the V3.1 reduced HSD Newton system
 # the small instances use the stable core path (the exact-preconditioner
 # gate, psipm_stable_preconditioner.py:202-207, would otherwise switch it off)
 OPTIONS = dict(full_preconditioner_row_threshold=10)
@@ -130,6 +131,8 @@ def main():
 
     if args.only in (None, "hsd_m1600"):
         make_hsd(PS, synthetic)
+    if args.only in (None, "hsd_newton_m1600"):
+        make_hsd_newton(synthetic)
 
 
 def make_hsd(PS, synthetic):
@@ -161,6 +164,102 @@ def make_hsd(PS, synthetic):
     path = os.path.join(HERE, "hsd_m1600.npz")
     np.savez_compressed(path, **out)
     print(f"hsd_m1600: iterations {[int(out[f'c{i}_iterations']) for i in range(3)]} "
+          f"-> {os.path.getsize(path) / 1e6:.2f} MB")
+
+
+def hsd_newton_inputs(A, b, rng):
+    """Seeded HSD iterate, embedding and boxes for one active-column set (shared
+    with the tests, which rebuild the same D from the stored iterate)."""
+    m, n = A.shape
+    boxed = rng.random(n) < 0.3
+    tau, kappa = 0.8, 0.3
+    x = rng.uniform(0.1, 2.0, n)
+    z = rng.uniform(0.1, 2.0, n)
+    upper = np.where(boxed, (x + rng.uniform(0.2, 2.0, n)) / tau, np.inf)
+    w = np.where(boxed, rng.uniform(0.1, 2.0, n), 0.0)
+    bar_b = b - A @ x / tau
+    bar_c = rng.standard_normal(n)
+    bar_g = float(rng.standard_normal())
+    return dict(x=x, z=z, w=w, upper=upper, tau=tau, kappa=kappa, bar_b=bar_b, bar_c=bar_c, bar_g=bar_g)
+
+
+def hsd_weights(x, z, w, upper, tau, rho, floor):
+    """D as the HSD step loop forms it (psipm_v3_1_hsd.py:1694-1695, 1718-1721)."""
+    boxed = np.isfinite(upper)
+    slack = np.ones_like(x)
+    slack[boxed] = upper[boxed] * tau - x[boxed]
+    ratio = np.zeros_like(x)
+    ratio[boxed] = w[boxed] / slack[boxed]
+    return 1.0 / np.maximum(rho + z / x + ratio, floor), slack
+
+
+def make_hsd_newton(synthetic):
+    """V3.1 HSDNewtonSystem (psipm_v3_1_hsd.py:1066-1264) over the reference's
+    StableColumnPreconditioner: two systems (the second at a moved iterate, so the
+    preconditioner's lagged-reuse policy runs), each with an affine direction
+    and a corrector direction shaped like the step loop's (:1734-1791)."""
+    import psipm_v3_1_hsd as H
+
+    lp = synthetic.random_lp(1600, 4800, seed=6)
+    A, b = lp.A.tocsc(), lp.b
+    m, n = A.shape
+    c = lp.c
+    rng = np.random.default_rng(41)
+    # growth_amortization 0 makes the core-growth rule (:954-984) independent of
+    # the measured PCG and factor times, so the fixture is reproducible
+    options = H.V3Options(generic_preconditioner="stable", generic_growth_amortization=0.0)
+    pre = H.StableColumnPreconditioner(A, options)
+    stats = H.LinearStats()
+    base = hsd_newton_inputs(A, b, rng)
+    out = dict(A_data=A.data, A_indices=A.indices, A_indptr=A.indptr, A_shape=np.array(A.shape), c=c, b=b,
+               upper=base["upper"], delta=options.delta, eta=options.eta, zeta=options.zeta,
+               rho=options.rho, floor=options.regularization_floor, pcg_tolerance=1e-10,
+               pcg_max_iterations=options.pcg_max_iterations,
+               growth_amortization=options.generic_growth_amortization)
+    for sys_i in range(2):
+        it = dict(base)
+        if sys_i:
+            boxed = np.isfinite(base["upper"])
+            it["x"] = base["x"] * np.where(boxed, 1.0, np.exp(rng.uniform(-0.5, 0.5, n)))
+            it["z"] = base["z"] * np.exp(rng.uniform(-0.5, 0.5, n))
+        D, slack = hsd_weights(it["x"], it["z"], it["w"], it["upper"], it["tau"], options.rho,
+                               options.regularization_floor)
+        state = H.HSDState(x=it["x"], y=np.zeros(m), z=it["z"], w=it["w"], tau=it["tau"], kappa=it["kappa"],
+                           theta=1.0, x_center=it["x"].copy(), y_center=np.zeros(m), tau_center=it["tau"],
+                           theta_center=1.0)
+        emb = H.HSDEmbedding(bar_b=it["bar_b"], bar_c=it["bar_c"], bar_g=it["bar_g"], alpha=1.0)
+        system = H.HSDNewtonSystem(A, c, it["upper"], b, D, options.delta, options.eta, state, emb, pre, 1e-10,
+                                   options, np.inf, stats)
+        boxed = np.isfinite(it["upper"])
+        rd, rp = rng.standard_normal(n), rng.standard_normal(m)
+        rg, rn = float(rng.standard_normal()), float(rng.standard_normal())
+        affine_rhs = (-rd, -rp, -rg, -rn, -it["x"] * it["z"], np.where(boxed, -slack * it["w"], 0.0),
+                      -it["tau"] * it["kappa"])
+        aff = system.direction(*affine_rhs)
+        ds = np.zeros(n)
+        ds[boxed] = it["upper"][boxed] * aff[4] - aff[0][boxed]
+        smu = 0.1 * float(it["x"] @ it["z"]) / n
+        corr_rhs = (np.zeros(n), np.zeros(m), 0.0, 0.0, smu - aff[0] * aff[2],
+                    np.where(boxed, smu - ds * aff[3], 0.0), smu - aff[4] * aff[6])
+        cor = system.direction(*corr_rhs)
+        out[f"s{sys_i}_x"], out[f"s{sys_i}_z"] = it["x"], it["z"]
+        for key in ("w", "tau", "kappa", "bar_b", "bar_c", "bar_g"):
+            out[f"s{sys_i}_{key}"] = it[key]
+        out[f"s{sys_i}_D"] = D
+        out[f"s{sys_i}_core"] = pre.impl.core.copy()
+        out[f"s{sys_i}_n_fact"] = pre.impl.n_fact
+        for d_i, (rhs, res) in enumerate(((affine_rhs, aff), (corr_rhs, cor))):
+            tag = f"s{sys_i}d{d_i}"
+            for k, v in enumerate(rhs):
+                out[f"{tag}_rhs{k}"] = v
+            for k, name in enumerate(("dx", "dy", "dz", "dw", "dtau", "dtheta", "dkappa", "ok")):
+                out[f"{tag}_{name}"] = res[k]
+        out[f"s{sys_i}_stats"] = np.array([stats.solves, stats.iterations, stats.max_iterations, stats.matvecs,
+                                           stats.failures])
+    path = os.path.join(HERE, "hsd_newton_m1600.npz")
+    np.savez_compressed(path, **out)
+    print(f"hsd_newton_m1600: stats {out['s1_stats'].tolist()} ok "
+          f"{[bool(out[f's{i}d{j}_ok']) for i in range(2) for j in range(2)]} "
           f"-> {os.path.getsize(path) / 1e6:.2f} MB")
 
 
