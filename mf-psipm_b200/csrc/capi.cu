@@ -1408,8 +1408,8 @@ __global__ void k_list_rows(int nrows, const int* __restrict__ rows, const int* 
     }
 }
 
-// long rows: one warp per 4,096-entry chunk, partial sums added with atomics
-// into the zeroed outputs of those rows
+// long rows: one warp per kLongRow-entry chunk, partial sums added with
+// atomics into the zeroed outputs of those rows
 __global__ void k_chunk_rows(int nchunks, const int* __restrict__ cbeg, const int* __restrict__ cend,
                              const int* __restrict__ crow, const int* __restrict__ idx,
                              const double* __restrict__ val, const double* __restrict__ v,
