@@ -169,6 +169,14 @@ int psipm_pcg(psipm_handle* h, const double* rhs, double tol, int32_t maxit, int
               int32_t replacement, double gap_tolerance, double* x, double* residual,
               double* alphas, double* betas, double* history, psipm_pcg_info* info);
 
+/* Wall-clock budget of every later PCG launch of this handle, in seconds
+ * (0: none).  The HSD variant tests it after each iteration's convergence
+ * test, like the deadline of psipm_v3_1_hsd.py:1054-1055, and returns the
+ * current x with ok = 0 when it has passed; the spectral variant stops with
+ * info = -8 (no reference code).  A budget of 1e-9 s stops after the first
+ * iteration, as the reference does when it starts past its deadline. */
+int psipm_set_pcg_budget(psipm_handle* h, double seconds);
+
 /* ---- H1 Newton solve ------------------------------------------------------------
  * w = r1/theta; rhs = r2 - A w; dy = PCG(rhs); dx = w + (A^T dy)/theta
  * (psipm_spectral_preconditioner.py:651-752 without the host policy). */

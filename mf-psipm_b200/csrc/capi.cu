@@ -97,6 +97,7 @@ struct psipm_handle {
     DevBuf<int> short_rows, long_rows, long_chunk_ptr, chunk_beg, chunk_end, chunk_row;
     int64_t short_nnz = 0;
     int n_short = 0, n_long = 0, n_chunks = 0, vw = 32;
+    long long pcg_budget_ns = 0;  // psipm_set_pcg_budget (0: none)
     DevBuf<long long> d_cand;
 
     // weights and scores
@@ -359,6 +360,7 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
     a.w = weights(h, tag);
     a.delta = (T)h->delta;
     a.gb = grid_barrier(h);
+    a.budget_ns = h->pcg_budget_ns;
     PrecLayout<P>& pc = a.pc;
     pc.m = (int)h->m;
     FactorStore<P>& fs = fstore(h, ptag);
@@ -1774,6 +1776,14 @@ int psipm_timer_stop(psipm_handle* h, double* seconds) {
         PSIPM_CUDA(cudaEventElapsedTime(&ms, h->tv0, h->tv1));
         *seconds = ms * 1e-3;
     });
+}
+
+int psipm_set_pcg_budget(psipm_handle* h, double seconds) {
+    if (!h || !(seconds >= 0.0)) return PSIPM_ERR_ARGUMENT;
+    // round up so that any positive budget stays positive; cap at ~290 years
+    const double ns = std::ceil(std::min(seconds, 9.0e18 * 1e-9) * 1e9);
+    h->pcg_budget_ns = (long long)ns;
+    return PSIPM_OK;
 }
 
 int psipm_set_profiling(psipm_handle* h, int32_t on) {

@@ -105,6 +105,7 @@ SIGNATURES = {
     "psipm_apply": (_I32, [_P, _P, _P]),
     "psipm_matvec": (_I32, [_P, _P, _P]),
     "psipm_pcg": (_I32, [_P, _P, _D, _I32, _I32, _I32, _D, _P, _P, _P, _P, _P, _P]),
+    "psipm_set_pcg_budget": (_I32, [_P, _D]),
     "psipm_solve": (_I32, [_P, _P, _P, _D, _I32, _I32, _I32, _D, _P, _P, _P, _P, _P, _P, _P]),
     "psipm_solve_dev": (_I32, [_P, _P, _P, _D, _I32, _I32, _I32, _D, _P, _P, _P]),
     "psipm_kernel_launches": (_I64, [_P]),

@@ -182,6 +182,10 @@ class NormalEquationsDevice:
                                        ptr(alphas), ptr(betas), ptr(history), ctypes.byref(info)))
         return self._result(x, info, alphas, betas, history, res)
 
+    def set_pcg_budget(self, seconds: float) -> None:
+        """Wall-clock budget of every later PCG launch (0: none), psipm_set_pcg_budget."""
+        self._check(self.lib.psipm_set_pcg_budget(self.h, float(seconds)))
+
     def solve(self, r1, r2, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100, gap_tolerance=0.1,
               want_residual=False):
         r1 = f64(r1)

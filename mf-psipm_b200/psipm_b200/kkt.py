@@ -761,10 +761,11 @@ class GpuStableColumnPreconditioner:
         One ``psipm_solve`` call: the right-hand side's SpMV, the PCG and the
         back-substitution run on the device; r1, r2 go in and dx, dy come out.
         Returns ``(dx, dy, iterations, matvecs, okay, elapsed)``; the deadline
-        limits the launch as in :func:`pcg_rows`.
+        bounds the launch as in :func:`pcg_rows`.
         """
         started = time.perf_counter()
-        dx, res = self.impl.dev.solve(r1, r2, rtol, _deadline_iterations(max_iterations, deadline), _lib.PCG_HSD)
+        dev = self.impl.dev
+        dx, res = _under_deadline(dev, deadline, lambda: dev.solve(r1, r2, rtol, int(max_iterations), _lib.PCG_HSD))
         return dx, res.x, res.iterations, res.matvecs, bool(res.ok), time.perf_counter() - started
 
 
@@ -777,16 +778,25 @@ def pcg_rows(preconditioner: GpuStableColumnPreconditioner, rhs, rtol, max_itera
     (psipm_v3_1_hsd.py:1136-1137).
     """
     started = time.perf_counter()
-    res = preconditioner.impl.dev.pcg(rhs, rtol, _deadline_iterations(max_iterations, deadline), _lib.PCG_HSD)
+    dev = preconditioner.impl.dev
+    res = _under_deadline(dev, deadline, lambda: dev.pcg(rhs, rtol, int(max_iterations), _lib.PCG_HSD))
     return res.x, res.iterations, res.matvecs, bool(res.ok), time.perf_counter() - started
 
 
-def _deadline_iterations(max_iterations, deadline) -> int:
-    """Iteration limit of one device PCG launch under the caller's deadline.
+def _under_deadline(dev, deadline, call):
+    """Run one device PCG call under the caller's ``time.perf_counter`` deadline.
 
     The reference tests the deadline after each iteration's convergence test
-    (psipm_v3_1_hsd.py:1054-1055), so a call that starts past it stops after
-    one iteration, converged or not.  The device PCG runs as one launch, so
-    the deadline is tested when it starts: one iteration if it has passed.
+    and then returns the current x as not converged (psipm_v3_1_hsd.py:1054-1055);
+    the device PCG does the same against a wall-clock budget
+    (``psipm_set_pcg_budget``), set here to the time left (at least 1 ns, so a
+    call that starts past its deadline stops after one iteration) and cleared
+    afterwards.
     """
-    return 1 if time.perf_counter() >= deadline and max_iterations > 0 else int(max_iterations)
+    if not np.isfinite(deadline):
+        return call()
+    dev.set_pcg_budget(max(deadline - time.perf_counter(), 1e-9))
+    try:
+        return call()
+    finally:
+        dev.set_pcg_budget(0.0)

@@ -123,6 +123,9 @@ class FakeDevice:
     def matvec(self, v):
         return self._H(np.asarray(v, dtype=float))
 
+    def set_pcg_budget(self, seconds):
+        self.pcg_budget = float(seconds)
+
     def solve(self, r1, r2, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100, gap_tolerance=0.1,
               want_residual=False):
         self._maybe_fail("solve")

@@ -135,10 +135,30 @@ def test_singular_border_is_shifted_and_reported(fixture):
     assert rel(got[1], want[1]) <= 1e-6
 
 
-def test_deadline_limits_the_launch():
-    """A call that starts past its deadline runs one iteration (psipm_v3_1_hsd.py:1054-1055)."""
-    from psipm_b200.kkt import _deadline_iterations
+def test_deadline_becomes_a_device_budget():
+    """A finite deadline is passed to the device PCG as the time left (at
+    least 1 ns: one iteration, as the reference when it starts past its deadline,
+    psipm_v3_1_hsd.py:1054-1055) and cleared afterwards; none is set without one."""
+    from types import SimpleNamespace as NS
 
-    assert _deadline_iterations(1000, np.inf) == 1000
-    assert _deadline_iterations(1000, 0.0) == 1
-    assert _deadline_iterations(0, 0.0) == 0
+    from psipm_b200.kkt import pcg_rows
+
+    class Dev:
+        def __init__(self):
+            self.budgets = []
+
+        def set_pcg_budget(self, seconds):
+            self.budgets.append(seconds)
+
+        def pcg(self, rhs, tol, maxit, variant):
+            return NS(x=np.zeros(3), iterations=1, matvecs=2, ok=False)
+
+    dev = Dev()
+    pre = NS(impl=NS(dev=dev))
+    assert pcg_rows(pre, np.ones(3), 1e-10, 50)[3] is False and dev.budgets == []
+    pcg_rows(pre, np.ones(3), 1e-10, 50, deadline=0.0)
+    assert dev.budgets == [1e-9, 0.0]
+    import time
+
+    pcg_rows(pre, np.ones(3), 1e-10, 50, deadline=time.perf_counter() + 100.0)
+    assert 99.0 < dev.budgets[2] <= 100.0 and dev.budgets[3] == 0.0
