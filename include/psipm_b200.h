@@ -62,7 +62,7 @@ typedef struct {
     int32_t n_beta;          /* entries written to betas[] */
     int32_t n_history;       /* entries written to history[] */
     int32_t refinements;     /* FP64 refinement sweeps (FP32_REFINED only) */
-    int32_t ok;              /* HSD variant: converged flag */
+    int32_t ok;              /* converged (spectral variant: info == 0) */
     double relative_residual;/* ||rhs - H x|| / max(1, ||rhs||) in FP64 */
     double seconds;          /* device time of the call (CUDA events) */
     double phase_seconds[4]; /* device time by phase: [0] H·p passes, [1] vector

@@ -858,6 +858,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T, P> a) {
         last_r = sqrt(fin);
         rel = last_r / scale;
         if (info > 0 && rel <= target) info = 0;
+        ok = info == 0;
     }
 done:
     if (hsd) rel = scale > 0.0 ? last_r / scale : 0.0;
