@@ -35,3 +35,36 @@ def test_binding_signatures_cover_header():
     from psipm_b200 import _lib
 
     assert set(_lib.SIGNATURES) == set(declared_functions())
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    """include/psipm_b200.h is plain C99: a C caller compiles against it, links
+    the library and gets the documented argument error (no GPU involved)."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        import pytest
+
+        pytest.skip("gcc not available")
+    src = tmp_path / "caller.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "psipm_b200.h"
+int main(void) {
+    psipm_handle* h = 0;
+    int64_t colptr[2] = {0, 0};
+    int rc = psipm_create(0, 1, 0, colptr, 0, 0, 0, PSIPM_FP64, &h);
+    int rc2 = psipm_solve(0, 0, 0, 1e-8, 10, PSIPM_PCG_SPECTRAL, 100, 0.1, 0, 0, 0, 0, 0, 0, 0);
+    printf("%d %d %lld\n", rc, rc2, (long long)psipm_num_candidates(0));
+    psipm_destroy(0);
+    return (rc == PSIPM_ERR_ARGUMENT && rc2 == PSIPM_ERR_ARGUMENT) ? 0 : 1;
+}
+''')
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(LIB)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe), "-L", libdir, "-lpsipm_b200", f"-Wl,-rpath,{libdir}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.split() == ["-1", "-1", "-1"]
