@@ -721,6 +721,10 @@ class GpuStableColumnPreconditioner:
     def backend(self) -> str:
         return "stable-active-column-b200"
 
+    def close(self) -> None:
+        """Release the device handle (the reference's object has nothing to release)."""
+        self.impl.close()
+
     def factor(self, weights, delta) -> float:  # :902-921
         started = time.perf_counter()
         before = int(self.impl.n_fact)
