@@ -337,13 +337,23 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
         std::vector<int32_t>().swap(merged[p]);
         int64_t degLp = 0;
         for (int32_t i : Lp) degLp += nv[i];
-        // prune the adjacency of every variable of the new element
+        // prune the adjacency of every variable of the new element, and
+        // w(e) = |Le \ Lp| for the other elements touching Lp.  w(e) starts
+        // from |Le|, which never changes while e lives: a variable leaves Le
+        // only as a pivot (which absorbs e) or by merging into a variable of Le.
         for (int32_t i : Lp) {
             remove(i);
             std::vector<int32_t>& Ei = E[i];
             size_t w = 0;
-            for (int32_t e : Ei)
-                if (status[e] == ELEM) Ei[w++] = e;
+            for (int32_t e : Ei) {
+                if (status[e] != ELEM) continue;
+                Ei[w++] = e;
+                if (wstamp[e] != step) {
+                    wstamp[e] = step;
+                    wval[e] = esize[e];
+                }
+                wval[e] -= nv[i];
+            }
             Ei.resize(w);
             Ei.push_back(p);
             std::vector<int32_t>& Vi = V[i];
@@ -352,48 +362,40 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
                 if (status[v] == VAR && mark[v] != tag) Vi[w++] = v;
             Vi.resize(w);
         }
-        // |Le \ Lp| for the other elements touching Lp
-        for (int32_t i : Lp)
-            for (int32_t e : E[i]) {
-                if (e == p) continue;
-                if (wstamp[e] != step) {
-                    // |Le| never changes while e lives: a variable leaves Le only as
-                    // a pivot (which absorbs e) or by merging into a variable of Le
-                    wstamp[e] = step;
-                    wval[e] = esize[e];
-                }
-                wval[e] -= nv[i];
-            }
-        // approximate external degrees, aggressive absorption
-        for (int32_t i : Lp) {
-            int64_t dext = degLp - nv[i];
-            for (int32_t v : V[i]) dext += nv[v];
-            for (int32_t e : E[i]) {
-                if (e == p) continue;
-                if (wval[e] <= 0 && status[e] == ELEM) {
-                    status[e] = ABSORBED;  // e is a subset of Lp
-                    std::vector<int32_t>().swap(L[e]);
-                    continue;
-                }
-                if (status[e] == ELEM) dext += wval[e];
-            }
-            int64_t bound = deg[i] + degLp - nv[i];
-            deg[i] = std::max<int64_t>(0, std::min<int64_t>({dext, bound, (int64_t)n - eliminated}));
-        }
-        // supervariables: identical (V, E) among Lp.  The hash is a sum of
-        // mixed indices, so it needs no sorted lists; equal hashes are
+        // approximate external degrees, aggressive absorption, and the
+        // supervariable hash of each variable's final (V, E) lists.  An element
+        // with w(e) <= 0 is a subset of Lp and is absorbed by the first variable
+        // that meets it; w(e) is fixed for the step, so whether an element of
+        // E[i] survives the step is known when i is visited.  The hash is a sum
+        // of mixed indices, so it needs no sorted lists; equal hashes are
         // confirmed by marking one variable's lists and scanning the other's.
         hashes.clear();
         for (int32_t i : Lp) {
+            int64_t dext = degLp - nv[i];
+            uint64_t hl = 0;
+            for (int32_t v : V[i]) {
+                dext += nv[v];
+                hl += mix64((uint64_t)v);
+            }
             std::vector<int32_t>& Ei = E[i];
             size_t w = 0;
-            for (int32_t e : Ei)
-                if (status[e] == ELEM) Ei[w++] = e;
+            for (int32_t e : Ei) {
+                if (e != p) {
+                    if (status[e] != ELEM) continue;  // absorbed earlier in this pass
+                    if (wval[e] <= 0) {
+                        status[e] = ABSORBED;
+                        std::vector<int32_t>().swap(L[e]);
+                        continue;
+                    }
+                    dext += wval[e];
+                }
+                Ei[w++] = e;
+                hl += mix64((uint64_t)e ^ 0x5bd1e9955bd1e995ull);
+            }
             Ei.resize(w);
-            uint64_t h = (uint64_t)V[i].size() * 0x9e3779b97f4a7c15ull + (uint64_t)Ei.size();
-            for (int32_t v : V[i]) h += mix64((uint64_t)v);
-            for (int32_t e : Ei) h += mix64((uint64_t)e ^ 0x5bd1e9955bd1e995ull);
-            hashes.emplace_back(h, i);
+            int64_t bound = deg[i] + degLp - nv[i];
+            deg[i] = std::max<int64_t>(0, std::min<int64_t>({dext, bound, (int64_t)n - eliminated}));
+            hashes.emplace_back((uint64_t)V[i].size() * 0x9e3779b97f4a7c15ull + (uint64_t)w + hl, i);
         }
         std::sort(hashes.begin(), hashes.end());
         auto same_lists = [&](int32_t i, int32_t j) {
