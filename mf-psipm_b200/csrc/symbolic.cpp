@@ -337,7 +337,7 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
         std::vector<int32_t>().swap(merged[p]);
         int64_t degLp = 0;
         for (int32_t i : Lp) degLp += nv[i];
-        // prune the adjacency of every variable of the new element, and
+        // prune the element lists of the new element's variables, and
         // w(e) = |Le \ Lp| for the other elements touching Lp.  w(e) starts
         // from |Le|, which never changes while e lives: a variable leaves Le
         // only as a pivot (which absorbs e) or by merging into a variable of Le.
@@ -356,14 +356,11 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
             }
             Ei.resize(w);
             Ei.push_back(p);
-            std::vector<int32_t>& Vi = V[i];
-            w = 0;
-            for (int32_t v : Vi)
-                if (status[v] == VAR && mark[v] != tag) Vi[w++] = v;
-            Vi.resize(w);
         }
-        // approximate external degrees, aggressive absorption, and the
-        // supervariable hash of each variable's final (V, E) lists.  An element
+        // prune the variable lists (drop eliminated variables and those of Lp,
+        // now reached through p), approximate external degrees, aggressive
+        // absorption, and the supervariable hash of each variable's final
+        // (V, E) lists.  An element
         // with w(e) <= 0 is a subset of Lp and is absorbed by the first variable
         // that meets it; w(e) is fixed for the step, so whether an element of
         // E[i] survives the step is known when i is visited.  The hash is a sum
@@ -373,10 +370,15 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
         for (int32_t i : Lp) {
             int64_t dext = degLp - nv[i];
             uint64_t hl = 0;
-            for (int32_t v : V[i]) {
+            std::vector<int32_t>& Vi = V[i];
+            size_t wv = 0;
+            for (int32_t v : Vi) {
+                if (status[v] != VAR || mark[v] == tag) continue;
+                Vi[wv++] = v;
                 dext += nv[v];
                 hl += mix64((uint64_t)v);
             }
+            Vi.resize(wv);
             std::vector<int32_t>& Ei = E[i];
             size_t w = 0;
             for (int32_t e : Ei) {
@@ -395,7 +397,7 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
             Ei.resize(w);
             int64_t bound = deg[i] + degLp - nv[i];
             deg[i] = std::max<int64_t>(0, std::min<int64_t>({dext, bound, (int64_t)n - eliminated}));
-            hashes.emplace_back((uint64_t)V[i].size() * 0x9e3779b97f4a7c15ull + (uint64_t)w + hl, i);
+            hashes.emplace_back((uint64_t)wv * 0x9e3779b97f4a7c15ull + (uint64_t)w + hl, i);
         }
         std::sort(hashes.begin(), hashes.end());
         auto same_lists = [&](int32_t i, int32_t j) {
