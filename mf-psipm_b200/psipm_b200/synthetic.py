@@ -30,7 +30,7 @@ pure function of its arguments.
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import List, Optional
+from typing import List
 
 import numpy as np
 import scipy.sparse as sp
