@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <utility>
 
 namespace psipm {
@@ -450,6 +451,28 @@ void amd_order(const Graph& g, std::vector<int32_t>& order) {
     }
 }
 
+// Host threads for a symbolic analysis of `work` expanded-product keys: one
+// below 2^18, else up to 8.
+int host_threads(int64_t work) {
+    if (work < (int64_t(1) << 18)) return 1;
+    const unsigned hc = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(hc ? hc : 1u, 8u));
+}
+
+// f(thread, lo, hi) on `nthreads` contiguous ranges of [0, n), one per host
+// thread (the calling thread takes the first).  f must not throw.
+template <typename F>
+void run_chunks(int nthreads, int64_t n, F f) {
+    if (nthreads <= 1 || n <= 1) {
+        f(0, 0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(f, t, n * t / nthreads, n * (t + 1) / nthreads);
+    f(0, 0, n / nthreads);
+    for (auto& th : pool) th.join();
+}
+
 }  // namespace
 
 int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* rowidx,
@@ -802,56 +825,107 @@ int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* r
         double v;
     };
     // linearised front position: sn_rowptr-based column-major within the
-    // panel: panel_off[s] + rowpos * c + col  (row-major panel index)
-    std::vector<Key> keys;
-    keys.reserve((size_t)ncore * 8 + m);
-    std::vector<std::pair<int32_t, double>> col;
+    // panel: panel_off[s] + rowpos * c + col  (row-major panel index).
+    // Large analyses split the key generation, the supernode scatter and the
+    // per-supernode sorts over host threads; every thread owns a fixed range
+    // and writes fixed slots, so the result is the sequential one.
+    std::vector<int64_t> kofs(ncore + 1, 0);
     for (int64_t t = 0; t < ncore; ++t) {
-        int64_t kk = core[t];
-        col.clear();
-        for (int64_t a = colptr[kk]; a < colptr[kk + 1]; ++a)
-            col.emplace_back(S.iperm[rowidx[a]], val[a]);
-        std::sort(col.begin(), col.end());
-        for (size_t a = 0; a < col.size(); ++a)
-            for (size_t b = a; b < col.size(); ++b) {
-                int32_t j = col[a].first, i = col[b].first;  // j <= i
-                int32_t s = col2sn[j];
-                const int32_t* sr = S.sn_rows.data() + S.sn_rowptr[s];
-                int64_t rn = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
-                int32_t c = S.sn_first[s + 1] - S.sn_first[s];
-                int64_t rp;
-                if (i < S.sn_first[s + 1]) {
-                    rp = i - S.sn_first[s];
-                } else {
-                    const int32_t* it = std::lower_bound(sr + c, sr + rn, i);
-                    if (it == sr + rn || *it != i) return -12;
-                    rp = it - sr;
-                }
-                int64_t pos = S.panel_off[s] + rp * c + (j - S.sn_first[s]);
-                keys.push_back({pos, (int32_t)t, s, col[a].second * col[b].second});
-            }
+        const int64_t q = colptr[core[t] + 1] - colptr[core[t]];
+        kofs[t + 1] = kofs[t] + q * (q + 1) / 2;
     }
+    const int64_t ncol_keys = kofs[ncore];
+    std::vector<Key> keys((size_t)(ncol_keys + m));
+    const int nthreads = host_threads(ncol_keys + m);
+    std::vector<int> thread_rc(nthreads, 0);
+    run_chunks(nthreads, ncore, [&](int tid, int64_t lo, int64_t hi) {
+      try {
+        std::vector<std::pair<int32_t, double>> col;
+        for (int64_t t = lo; t < hi; ++t) {
+            int64_t kk = core[t];
+            col.clear();
+            for (int64_t a = colptr[kk]; a < colptr[kk + 1]; ++a)
+                col.emplace_back(S.iperm[rowidx[a]], val[a]);
+            std::sort(col.begin(), col.end());
+            int64_t out = kofs[t];
+            for (size_t a = 0; a < col.size(); ++a)
+                for (size_t b = a; b < col.size(); ++b) {
+                    int32_t j = col[a].first, i = col[b].first;  // j <= i
+                    int32_t s = col2sn[j];
+                    const int32_t* sr = S.sn_rows.data() + S.sn_rowptr[s];
+                    int64_t rn = S.sn_rowptr[s + 1] - S.sn_rowptr[s];
+                    int32_t c = S.sn_first[s + 1] - S.sn_first[s];
+                    int64_t rp;
+                    if (i < S.sn_first[s + 1]) {
+                        rp = i - S.sn_first[s];
+                    } else {
+                        const int32_t* it = std::lower_bound(sr + c, sr + rn, i);
+                        if (it == sr + rn || *it != i) {
+                            thread_rc[tid] = -12;
+                            return;
+                        }
+                        rp = it - sr;
+                    }
+                    int64_t pos = S.panel_off[s] + rp * c + (j - S.sn_first[s]);
+                    keys[out++] = {pos, (int32_t)t, s, col[a].second * col[b].second};
+                }
+        }
+      } catch (...) {
+        thread_rc[tid] = -14;  // host allocation failed
+      }
+    });
+    for (int rc : thread_rc)
+        if (rc) return rc;
     // every diagonal entry exists even without contributions
     for (int32_t i = 0; i < m; ++i) {
         int32_t s = col2sn[i];
         int32_t c = S.sn_first[s + 1] - S.sn_first[s];
         int64_t rp = i - S.sn_first[s];
-        keys.push_back({S.panel_off[s] + rp * c + rp, -1, s, 0.0});
+        keys[ncol_keys + i] = {S.panel_off[s] + rp * c + rp, -1, s, 0.0};
     }
     // order by (position, column): a stable counting sort by supernode (positions
     // of different supernodes do not interleave), then a sort inside each
-    // supernode's short run
+    // supernode's short run.  The scatter is stable across threads: thread t's
+    // keys of a supernode go after those of threads < t.
     {
+        const int64_t nk = (int64_t)keys.size();
+        std::vector<std::vector<int64_t>> cnt(nthreads, std::vector<int64_t>(ns + 1, 0));
+        run_chunks(nthreads, nk, [&](int tid, int64_t lo, int64_t hi) {
+            std::vector<int64_t>& c = cnt[tid];
+            for (int64_t q = lo; q < hi; ++q) ++c[keys[q].s];
+        });
         std::vector<int64_t> bptr(ns + 1, 0);
-        for (const Key& q : keys) ++bptr[q.s + 1];
-        for (int32_t t = 0; t < ns; ++t) bptr[t + 1] += bptr[t];
-        std::vector<Key> sorted(keys.size());
         {
-            std::vector<int64_t> f(bptr.begin(), bptr.end() - 1);
-            for (const Key& q : keys) sorted[f[q.s]++] = q;
+            int64_t run = 0;
+            for (int32_t t = 0; t < ns; ++t) {
+                bptr[t] = run;
+                for (int tid = 0; tid < nthreads; ++tid) {
+                    const int64_t v = cnt[tid][t];
+                    cnt[tid][t] = run;  // this thread's first slot for supernode t
+                    run += v;
+                }
+            }
+            bptr[ns] = run;
         }
+        std::vector<Key> sorted(keys.size());
+        run_chunks(nthreads, nk, [&](int tid, int64_t lo, int64_t hi) {
+            std::vector<int64_t>& f = cnt[tid];
+            for (int64_t q = lo; q < hi; ++q) sorted[f[keys[q].s]++] = keys[q];
+        });
         auto less = [](const Key& a, const Key& b) { return a.pos < b.pos || (a.pos == b.pos && a.k < b.k); };
-        for (int32_t t = 0; t < ns; ++t) std::sort(sorted.begin() + bptr[t], sorted.begin() + bptr[t + 1], less);
+        // supernode ranges of about equal key counts per thread
+        std::vector<int32_t> sbeg(nthreads + 1, ns);
+        sbeg[0] = 0;
+        for (int tid = 1, t = 0; tid < nthreads; ++tid) {
+            const int64_t goal = nk * tid / nthreads;
+            while (t < ns && bptr[t] < goal) ++t;
+            sbeg[tid] = t;
+        }
+        run_chunks(nthreads, nthreads, [&](int, int64_t lo, int64_t hi) {
+            for (int64_t part = lo; part < hi; ++part)
+                for (int32_t t = sbeg[part]; t < sbeg[part + 1]; ++t)
+                    std::sort(sorted.begin() + bptr[t], sorted.begin() + bptr[t + 1], less);
+        });
         keys.swap(sorted);
     }
     // distinct positions -> entries

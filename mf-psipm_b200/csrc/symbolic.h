@@ -81,7 +81,10 @@ struct SymbolicOptions {
 
 // Build the symbolic factor for the core columns `core` (sorted, global
 // column indices) of A given in CSC (colptr[n+1], rowidx[nnz], val[nnz]).
-// Returns 0 on success, a negative value on invalid input.
+// Returns 0 on success, a negative value on invalid input (-14: a host
+// allocation failed).  Analyses with more than 2^18 expanded-product keys build
+// the expanded product on up to 8 host threads; the result does not depend on
+// the thread count.
 int build_symbolic(int32_t m, int64_t n, const int64_t* colptr, const int32_t* rowidx,
                    const double* val, const int64_t* core, int64_t ncore,
                    const SymbolicOptions& opt, Symbolic& out);
