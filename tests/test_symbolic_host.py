@@ -186,3 +186,38 @@ def test_symbolic_structure(driver, golden, ordering):
             assert first[s] + S["ent_col"][de[i]] == i and rows[rowptr[s] + S["ent_rowpos"][de[i]]] == i
         checked += 1
     assert checked >= 10
+
+
+def test_threaded_expanded_product(driver):
+    """A core large enough (> 2^18 expanded-product keys) for the threaded
+    construction: repeated runs give identical arrays, and the expanded product
+    still assembles A_C diag(w) A_C' exactly."""
+    from psipm_b200 import synthetic
+
+    A = synthetic.grid_network(120, 160, seed=7).A.tocsc()
+    A.sum_duplicates()
+    A.sort_indices()
+    core = np.flatnonzero(np.diff(A.indptr) >= 2).astype(np.int64)
+    q = np.diff(A.indptr)[core]
+    assert int((q * (q + 1) // 2).sum()) + A.shape[0] > (1 << 18)
+    S1 = run_symbolic(driver, A, core)
+    S2 = run_symbolic(driver, A, core)
+    for name, _ in FIELDS:
+        assert np.array_equal(S1[name], S2[name]), name
+    S = S1
+    assert int(S["head"][0]) == 0
+    first, rowptr, rows = S["sn_first"], S["sn_rowptr"], S["sn_rows"]
+    ent_ptr = S["ent_ptr"]
+    j = first[S["ent_sn"]] + S["ent_col"]
+    i = rows[rowptr[S["ent_sn"]] + S["ent_rowpos"]]
+    w = np.random.default_rng(5).uniform(0.5, 2.0, core.size)
+    counts = np.diff(ent_ptr)
+    owner = np.repeat(np.arange(counts.size), counts)
+    vals = np.bincount(owner, weights=S["contrib_val"] * w[S["contrib_col"]], minlength=counts.size)
+    got = sp.coo_matrix((vals, (i, j)), shape=(A.shape[0],) * 2).tocsr()
+    Ac = A[:, core]
+    perm = S["perm"]
+    want = sp.tril((Ac @ sp.diags(w) @ Ac.T).tocsc()[perm][:, perm]).tocsr()
+    diff = abs(got - want)
+    assert diff.max() <= 1e-12 * max(1.0, abs(want).max())
+    assert got.nnz >= want.nnz
