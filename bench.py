@@ -19,7 +19,10 @@ Keys of the JSON line:
              its launches / its CUDA-event time, against the measured HBM
              copy bandwidth;
 * cpu_baseline  the CPU oracle (reference algorithm, SuperLU stand-in
-             factor) on a bounded sample of the same LP, scaled to one solve.
+             factor) timed on a bounded sample of the same LP (its first K
+             outer iterations), next to the device's time for the same K
+             outer iterations (same_work); the reference's complete solve,
+             measured once elsewhere, is reported beside it, labelled.
 
 ``--impl reference`` times that CPU implementation alone (rank 0).
 Multi-GPU: one process per GPU (torchrun), each solving its own seeded
@@ -173,17 +176,27 @@ def flush_l2():
     del buf
 
 
-def calibrated(seconds, args):
-    cal = CALIBRATION.get((args.rows, args.cols))
-    if cal is None or args.cpu_sample_outer != cal["sample_outer"]:
-        return None, None
-    value = seconds * cal["full_seconds"] / cal["sample_seconds"]
-    text = (f"oracle (reference algorithm, SuperLU stand-in factor) on the first {cal['sample_outer']} "
-            f"PS-IPM outer iterations of the same LP ({seconds:.1f} s here), scaled by the ratio "
-            f"{cal['full_seconds']:.1f} s / {cal['sample_seconds']:.2f} s of a complete run of the same "
-            f"oracle to 1e-8 ({cal['outer']} outer / {cal['inner']} inner / {cal['pcg']} PCG iterations) "
-            f"to its first {cal['sample_outer']} outer iterations")
-    return value, text
+REFERENCE_RESULT = os.path.join(ROOT, "tests", "golden", "grid_200x250_result.json")
+
+
+def reference_full_solve(args):
+    """The unmodified reference's complete solve of this LP to 1e-8, measured
+    once by tests/golden/make_golden.py (SuperLU stand-in factor) on the
+    machine named in the file; reported beside the bounded sample, never as
+    the sample's value."""
+    if (args.rows, args.cols) != (200, 250) or not os.path.exists(REFERENCE_RESULT):
+        return None
+    with open(REFERENCE_RESULT) as f:
+        d = json.load(f)
+    return {"seconds": d["seconds"], "cpu_count": d.get("cpu_count"), "outer_iterations": d["outer_iter"],
+            "pcg_iterations": d["pcg_iterations"], "objective": d["obj"], "status": d["status"],
+            "note": "measured once by tests/golden/make_golden.py, not on this host"}
+
+
+def sample_text(args, seconds):
+    return (f"oracle (reference algorithm, SuperLU stand-in factor) on the first {args.cpu_sample_outer} "
+            f"PS-IPM outer iterations of the same LP: {seconds:.2f} s measured here; the device's time for "
+            f"the same {args.cpu_sample_outer} outer iterations is in same_work")
 
 
 def run_reference(args, rank, world):
@@ -197,34 +210,25 @@ def run_reference(args, rank, world):
         if step >= args.warmup:
             samples.append(seconds)
     mean = sum(samples) / len(samples)
-    value, text = calibrated(mean, args)
     line = {
-        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": mean, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * mean, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "tol": args.tol},
-        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": text},
-        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": WORKLOAD, "tol": args.tol,
+                   "sample": f"first {args.cpu_sample_outer} PS-IPM outer iterations (bounded sample; a "
+                             f"complete solve takes tens of minutes on the CPU)"},
+        "cpu_baseline": {"value": mean, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": sample_text(args, mean)},
+        "e2e": {"value": mean, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_full_solve": reference_full_solve(args),
     }
     return line
-
-
-# A complete oracle solve of the 200x250 network LP to 1e-8 (8-core Xeon @
-# 2.7 GHz, OpenBLAS threads = 8): 2184.7 s, 14 outer / 38 inner iterations,
-# 10,736 PCG iterations; the same first two outer iterations took 7.61 s.
-# The bounded sample measured on the bench host is scaled by that ratio,
-# because the per-iteration cost grows roughly 20x over a solve (the core and
-# its factor grow), so a linear scale-up of the first iterations would
-# understate the CPU time by about that factor.
-CALIBRATION = {(200, 250): dict(full_seconds=2184.7, sample_seconds=7.61, sample_outer=2,
-                                outer=14, inner=38, pcg=10736)}
 
 
 def run_ours(args, rank, world, local_rank):
     import torch
 
-    from psipm_b200 import ipm
-    from psipm_b200.ipm_device import psipm_solve_resident
+    from psipm_b200.ipm_device import psipm_solve_resident, solve_standard
     from psipm_b200.device import NormalEquationsDevice
     from psipm_b200.replicas import max_over_ranks
     from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner
@@ -273,12 +277,12 @@ def run_ours(args, rank, world, local_rank):
     # ---- end to end through the public API, host buffers ----------------------
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sol_e2e, solver_e2e = ipm.solve_standard(lp, tol=args.tol, device=local_rank)
+    sol_e2e, solver_e2e = solve_standard(lp, tol=args.tol, device=local_rank)
     x_host = np.array(sol_e2e.x)
     torch.cuda.synchronize()
     e2e = time.perf_counter() - t0
     h2d = (8 * (n + 1) + 12 * lp.A.nnz) + solver_e2e.h2d_bytes
-    d2h = 8 * solver_e2e.candidates.size + solver_e2e.d2h_bytes + 8 * x_host.size * 0
+    d2h = 8 * solver_e2e.candidates.size + solver_e2e.d2h_bytes
     solver_e2e.close()
     e2e = max_over_ranks(e2e)
     peak, peak_kind = measured_peaks()
@@ -299,9 +303,20 @@ def run_ours(args, rank, world, local_rank):
         sol0 = sols[-1]
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            seconds, inner, _ = cpu_oracle_sample(lp, args.tol, args.cpu_sample_outer, seconds_limit=1e9)
-            value, text = calibrated(seconds, args)
-            cpu = {"value": value, "unit": "s", "cores": blas_threads(), "kind": "port", "sample": text}
+            # the same bounded work on both sides: the first K outer iterations
+            torch.cuda.synchronize()
+            dev.timer_start()
+            solver_s = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev)
+            sol_s = psipm_solve_resident(lp, solver_s, tol=args.tol, max_outer=args.cpu_sample_outer)
+            gpu_same = dev.timer_stop()
+            seconds, inner, sol_c = cpu_oracle_sample(lp, args.tol, args.cpu_sample_outer, seconds_limit=1e9)
+            cpu = {"value": seconds, "unit": "s", "cores": blas_threads(), "kind": "port",
+                   "sample": sample_text(args, seconds),
+                   "same_work": {"outer_iterations": args.cpu_sample_outer, "cpu_s": seconds, "gpu_s": gpu_same,
+                                 "ratio": seconds / gpu_same if gpu_same > 0 else None,
+                                 "cpu_inner_iterations": int(sol_c.inner_iter),
+                                 "gpu_inner_iterations": int(sol_s.inner_iter)},
+                   "reference_full_solve": reference_full_solve(args)}
         line = {
             "metric": METRIC, "value": per_step, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * per_step, "higher_is_better": False,

@@ -133,6 +133,15 @@ int psipm_scores(psipm_handle* h, double fill_weight, double* scores, double* di
 int psipm_refresh_core(psipm_handle* h, int64_t target, double retention, int32_t stable,
                        const int64_t* mandatory_local, int64_t nmandatory,
                        int64_t* core_out, int64_t* ncore, double* retained);
+/* Straddling ties of the top-k selections (psipm_refresh_core, psipm_top_k).
+ * The reference selects with np.argpartition (psipm_stable_preconditioner.py:
+ * 97-110), whose pick among equal scores that straddle the cut depends on
+ * NumPy's build; this library takes them by ascending candidate index.  A
+ * selection "straddles" when the keys equal to its threshold outnumber the
+ * slots left for them.  out[4] = {selections that straddled (cumulative),
+ * tied keys at the last straddling threshold, slots they competed for,
+ * selections run (cumulative)}. */
+int psipm_tie_info(const psipm_handle* h, int64_t* out);
 /* Install an explicit core (sorted global column indices). */
 int psipm_set_core(psipm_handle* h, const int64_t* core, int64_t ncore);
 /* Top-`count` candidates among those with mask[i]!=0 (NULL mask: all) by
@@ -241,6 +250,24 @@ int psipm_ipm_targets(psipm_handle* h, int32_t kind, const double* params);
 int psipm_ipm_newton(psipm_handle* h, int32_t corrector, double tol, int32_t maxit,
                      int32_t variant, int32_t replacement, double gap_tolerance, double* alphas,
                      double* betas, double* history, int32_t* finite, psipm_pcg_info* info);
+/* Starting point on the device (_starting_point, psipm_active_pool.py:4122-4304,
+ * the default legacy projection).  With theta = 1 and delta = 1 factored
+ * (psipm_factor after the caller's policy chose the core), two projections:
+ * psipm_ipm_start_solve(which = 0) solves with r1 = 0, r2 = b and keeps
+ * x = A^T dy; which = 1 solves with r1 = 0, r2 = A c and keeps y = dy
+ * (alphas/betas/history/info and *finite as in psipm_ipm_newton).  Then
+ * psipm_ipm_start(solved) forms the start in the iterate: solved = 0 (a
+ * factorisation or a projection failed) starts from x = y = 0; non-finite x or
+ * y is replaced by zeros; the primal bound shifts, the dual estimate
+ * r = c - A^T y (y scaled by 0.95 when |r| < 0.05 |c|), the dual slack shifts,
+ * the complementarity-levelling shifts and the boxed projection follow the
+ * reference.  Sums fold block partials in a fixed order (the same start on
+ * every run).  out[5] (may be NULL) = {xshift1, zshift1, xshift2, zshift2,
+ * 1 if y was scaled}. */
+int psipm_ipm_start_solve(psipm_handle* h, int32_t which, double tol, int32_t maxit, int32_t variant,
+                          int32_t replacement, double gap_tolerance, double* alphas, double* betas,
+                          double* history, int32_t* finite, psipm_pcg_info* info);
+int psipm_ipm_start(psipm_handle* h, int32_t solved, double* out);
 /* Step to the boundary (_step_to_boundary, :1831-1837) along d = D (with_corrector
  * = 0) or d = D + gamma C: out[0] = min(1, min_{pos,dx<0} -x/dx, min_{box,ds<0} -s/ds),
  * out[1] = min(1, min_{pos,dz<0} -z/dz, min_{box,dw<0} -w/dw); ds = -dx. */
@@ -292,6 +319,15 @@ int psipm_timer_start(psipm_handle* h);
 int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t* stamps, int32_t cap,
                             int32_t* count, int32_t* barrier_ns);
 int psipm_timer_stop(psipm_handle* h, double* seconds);
+/* Timeout path of the persistent kernels' grid barrier, without a fault:
+ * `count` barriers with a poll limit of `polls` per wait, where block
+ * `skip_block` (-1: none) returns without arriving, so the other blocks' first
+ * wait runs out and sets the handle's timeout flag; every later wait then gives
+ * up within a few polls.  Returns PSIPM_ERR_TIMEOUT when a wait ran out (the
+ * handle stays usable), PSIPM_OK otherwise; *seconds is the host time of the
+ * launch. */
+int psipm_debug_barrier_timeout(psipm_handle* h, int32_t count, int32_t polls, int32_t skip_block,
+                                double* seconds);
 /* Shape of the current symbolic factor by height level (out[8 * l + .] for
  * l < min(cap, *nlevels)): {supernodes, fused single-warp supernodes,
  * supernodes cut into GEMV tasks, forward tasks, backward tasks,
@@ -318,9 +354,13 @@ int psipm_set_profiling(psipm_handle* h, int32_t on);
  * (PSIPM_ERR_ARGUMENT otherwise).  The kernels run on `stream` (a
  * cudaStream_t, NULL for the default stream) and the call returns without
  * waiting for them.  The first call on a device looks up the array's device
- * address and must come before any stream capture.  All calls share the one
- * array and it keeps the last call's contents (each call writes what it
- * reads, nothing needs clearing); calls whose kernels overlap on the GPU race. */
+ * address and must come before any stream capture; calls must not cross a
+ * cudaDeviceReset of that device (the cached address would be stale).  All
+ * calls share the one array and it keeps the last call's contents (each call
+ * writes what it reads, nothing needs clearing); calls whose kernels overlap
+ * on the GPU race.  A launch error already pending in the caller's context
+ * makes the call return PSIPM_ERR_CUDA without launching (the error stays
+ * pending). */
 #define PSIPM_STATIC_SCRATCH_MAX (1ll << 20)
 int psipm_normal_matvec_static(int64_t m, int64_t n, const int32_t* at_ptr, const int32_t* at_idx,
                                const double* at_val, const int32_t* a_ptr, const int32_t* a_idx,

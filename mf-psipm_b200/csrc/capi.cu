@@ -176,6 +176,9 @@ struct psipm_handle {
     DevBuf<int> eq, eqscan;
     DevBuf<unsigned int> hist;
     DevBuf<unsigned long long> counter;
+    // straddling ties (keys equal to the selection threshold outnumber the
+    // slots left for them): cumulative count, and the last one's sizes
+    int64_t tie_straddles = 0, tie_tied = 0, tie_slots = 0, selections = 0;
 };
 
 namespace {
@@ -773,6 +776,7 @@ int factor_numeric(psipm_handle* h, double delta, int start_shift) {
 void select_top(psipm_handle* h, const double* score, const unsigned char* mask, int64_t nsc,
                 int64_t count, unsigned char* out_flag) {
     if (count <= 0 || nsc == 0) return;
+    ++h->selections;
     cudaStream_t st = h->stream;
     h->counter.reserve(1);
     PSIPM_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(unsigned long long), st));
@@ -822,6 +826,11 @@ void select_top(psipm_handle* h, const double* score, const unsigned char* mask,
         int v = eqh[i];
         eqh[i] = acc;
         acc += v;
+    }
+    if (acc > need) {  // the cut falls inside a run of equal keys: the index rule decides
+        ++h->tie_straddles;
+        h->tie_tied = acc;
+        h->tie_slots = need;
     }
     h->eqscan.upload(eqh, st);
     LAUNCH(h, k_mark_ties<<<blocks_for(nsc, 256), 256, 0, st>>>(nsc, h->eq.p, h->eqscan.p, need, out_flag));
@@ -1279,6 +1288,15 @@ int psipm_refresh_core(psipm_handle* h, int64_t target, double retention, int32_
     });
 }
 
+int psipm_tie_info(const psipm_handle* h, int64_t* out) {
+    if (!h || !out) return PSIPM_ERR_ARGUMENT;
+    out[0] = h->tie_straddles;
+    out[1] = h->tie_tied;
+    out[2] = h->tie_slots;
+    out[3] = h->selections;
+    return PSIPM_OK;
+}
+
 int psipm_set_core(psipm_handle* h, const int64_t* core, int64_t ncore) {
     if (ncore < 0 || (ncore && !core)) return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
@@ -1725,7 +1743,8 @@ int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t
             int iters = 1000;
             long long* op = out.p;
             GridBarrier gb = grid_barrier(h);
-            void* bargs[] = {&iters, &op, &gb};
+            int skip = -1;
+            void* bargs[] = {&iters, &op, &gb, &skip};
             prepare_barrier(h);
             PSIPM_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_probe, dim3(h->coop_blocks),
                                                    dim3(kPcgThreads), bargs, 0, h->stream));
@@ -1735,6 +1754,29 @@ int psipm_debug_apply_trace(psipm_handle* h, const double* r, double* z, int64_t
             PSIPM_CUDA(cudaStreamSynchronize(h->stream));
             *barrier_ns = (int32_t)(ns / iters);
         }
+    });
+}
+
+int psipm_debug_barrier_timeout(psipm_handle* h, int32_t count, int32_t polls, int32_t skip_block,
+                                double* seconds) {
+    if (!h || count <= 0 || polls <= 0 || !seconds) return PSIPM_ERR_ARGUMENT;
+    *seconds = 0.0;
+    return guarded(h, [&]() {
+        require(skip_block < h->coop_blocks, PSIPM_ERR_ARGUMENT, "skip_block outside the grid");
+        DevBuf<long long> out;
+        out.zero(1, h->stream);
+        long long* op = out.p;
+        GridBarrier gb = grid_barrier(h);
+        gb.polls = (unsigned int)polls;
+        int skip = skip_block;
+        void* bargs[] = {&count, &op, &gb, &skip};
+        prepare_barrier(h);
+        const auto t0 = std::chrono::steady_clock::now();
+        PSIPM_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_probe, dim3(h->coop_blocks),
+                                               dim3(kPcgThreads), bargs, 0, h->stream));
+        ++h->launches;
+        PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     });
 }
 
@@ -2026,6 +2068,124 @@ int psipm_ipm_newton(psipm_handle* h, int32_t corrector, double tol, int32_t max
         PSIPM_CUDA(cudaStreamSynchronize(st));
         *finite = bad ? 0 : 1;
         if (info) *info = local;
+    });
+}
+
+int psipm_ipm_start_solve(psipm_handle* h, int32_t which, double tol, int32_t maxit, int32_t variant,
+                          int32_t replacement, double gap_tolerance, double* alphas, double* betas, double* history,
+                          int32_t* finite, psipm_pcg_info* info) {
+    if (maxit < 0 || !finite || (which != 0 && which != 1)) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        ipm_require(h);
+        require(h->have_factor, PSIPM_ERR_STATE, "solve before a successful factor");
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        const int64_t n = h->n, m = h->m;
+        PSIPM_CUDA(cudaMemsetAsync(I.r1.p, 0, n * sizeof(double), st));
+        // which 0: r2 = b, x = A^T dy (= dx at theta = 1, r1 = 0); which 1: r2 = A c, y = dy
+        if (which == 1) a_times(h, I.c.p, I.ax.p);
+        psipm_pcg_info local;
+        const double* dyd = nullptr;
+        solve_device(h, I.r1.p, which == 0 ? I.b.p : I.ax.p, tol, maxit, variant, replacement, gap_tolerance,
+                     I.dx.p, &local, &dyd);
+        PSIPM_CUDA(cudaMemcpyAsync(which == 0 ? I.x.p : I.y.p, which == 0 ? I.dx.p : dyd,
+                                   (which == 0 ? n : m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        PSIPM_CUDA(cudaMemsetAsync(I.flag.p, 0, sizeof(int), st));
+        LAUNCH(h, k_start_finite<<<blocks_for(std::max(n, m), kIpmThreads), kIpmThreads, 0, st>>>(
+                      n, m, I.dx.p, dyd, I.flag.p));
+        int bad = 0;
+        PSIPM_CUDA(cudaMemcpyAsync(&bad, I.flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        copy_out(h, alphas, h->alphas.p, local.n_alpha);
+        copy_out(h, betas, h->betas.p, local.n_beta);
+        copy_out(h, history, h->history.p, local.n_history);
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        *finite = bad ? 0 : 1;
+        if (info) *info = local;
+    });
+}
+
+int psipm_ipm_start(psipm_handle* h, int32_t solved, double* out) {
+    return guarded(h, [&]() {
+        ipm_require(h);
+        IpmStore& I = h->ipm;
+        cudaStream_t st = h->stream;
+        const int64_t n = h->n, m = h->m;
+        const int g = ipm_grid(h, std::max(n, m));
+        DevBuf<double> part, xl, xu, r;
+        part.reserve((size_t)kStartSlots * g);
+        xl.reserve(n);
+        xu.reserve(n);
+        r.reserve(n);
+        std::vector<double> hp((size_t)kStartSlots * g);
+        // fold slot k of the last kernel's partials in block order
+        auto fold = [&](int nslots) {
+            read_back(h, hp.data(), part.p, nslots * g);
+        };
+        auto sum_of = [&](int k) {
+            double v = 0.0;
+            for (int b = 0; b < g; ++b) v += hp[(size_t)k * g + b];
+            return v;
+        };
+        auto max_of = [&](int k) {
+            double v = 0.0;
+            for (int b = 0; b < g; ++b) v = std::max(v, hp[(size_t)k * g + b]);
+            return v;
+        };
+        if (!solved) {  // factorisation or a projection failed: x = y = 0 (:4182-4187)
+            PSIPM_CUDA(cudaMemsetAsync(I.x.p, 0, n * sizeof(double), st));
+            PSIPM_CUDA(cudaMemsetAsync(I.y.p, 0, m * sizeof(double), st));
+        }
+        // non-finite x or y is replaced by zeros (:4190-4193)
+        for (int pass = 0; pass < 2; ++pass) {
+            LAUNCH(h, k_start_bounds<<<g, kIpmThreads, 0, st>>>(n, m, I.x.p, I.y.p, I.u.p, I.pos.p, I.box.p, xl.p,
+                                                                 xu.p, part.p));
+            fold(4);
+            const bool xbad = max_of(0) != 0.0, ybad = max_of(3) != 0.0;
+            if (!xbad && !ybad) break;
+            require(pass == 0, PSIPM_ERR_BOUNDS, "starting point: zeroed x or y still not finite");
+            if (xbad) PSIPM_CUDA(cudaMemsetAsync(I.x.p, 0, n * sizeof(double), st));
+            if (ybad) PSIPM_CUDA(cudaMemsetAsync(I.y.p, 0, m * sizeof(double), st));
+        }
+        const double xinfeas = std::max(max_of(1), max_of(2));
+        const double xshift1 = 1.0 + 1.5 * xinfeas;
+        // dual estimate (:4200-4206)
+        spmv_csr(h, n, h->nnz, h->at_ptr.p, h->at_idx.p, h->at_val.p, I.y.p, I.aty.p);
+        LAUNCH(h, k_start_dual_norms<<<g, kIpmThreads, 0, st>>>(n, I.c.p, I.aty.p, r.p, part.p));
+        fold(2);
+        const double cnorm = std::sqrt(sum_of(0));
+        int scaled = 0;
+        if (cnorm > 0.0 && std::sqrt(sum_of(1)) < 0.05 * cnorm) {
+            LAUNCH(h, k_start_scale<<<blocks_for(m, kIpmThreads), kIpmThreads, 0, st>>>(m, 0.95, I.y.p));
+            spmv_csr(h, n, h->nnz, h->at_ptr.p, h->at_idx.p, h->at_val.p, I.y.p, I.aty.p);
+            LAUNCH(h, k_start_dual_norms<<<g, kIpmThreads, 0, st>>>(n, I.c.p, I.aty.p, r.p, part.p));
+            scaled = 1;
+        }
+        const int c_zero = cnorm == 0.0;
+        LAUNCH(h, k_start_slacks<<<g, kIpmThreads, 0, st>>>(n, r.p, xshift1, c_zero, I.pos.p, I.box.p, xl.p, xu.p,
+                                                             I.z.p, I.w.p, part.p));
+        fold(2);
+        const double zinfeas = std::max(max_of(0), max_of(1));
+        const double zshift1 = c_zero ? 0.0 : 1.0 + 1.5 * zinfeas;
+        LAUNCH(h, k_start_sums<<<g, kIpmThreads, 0, st>>>(n, zshift1, I.pos.p, I.box.p, xl.p, xu.p, I.z.p, I.w.p,
+                                                           part.p));
+        fold(6);
+        const double xsum = 1.0 + sum_of(0) + sum_of(1);
+        const double zsum = 1.0 + sum_of(2) + sum_of(3);
+        const double mu0 = 1.0 + sum_of(4) + sum_of(5);
+        double xshift2 = zsum > 0.0 ? 0.5 * mu0 / zsum : 0.0;
+        double zshift2 = xsum > 0.0 ? 0.5 * mu0 / xsum : 0.0;
+        if (!(std::isfinite(xshift2) && xshift2 > 0.0)) xshift2 = 0.0;
+        if (!(std::isfinite(zshift2) && zshift2 > 0.0)) zshift2 = 0.0;
+        LAUNCH(h, k_start_final<<<blocks_for(n, kIpmThreads), kIpmThreads, 0, st>>>(
+                      n, xshift2, zshift2, I.u.p, I.pos.p, I.box.p, xl.p, xu.p, I.x.p, I.z.p, I.w.p));
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        if (out) {
+            out[0] = xshift1;
+            out[1] = zshift1;
+            out[2] = xshift2;
+            out[3] = zshift2;
+            out[4] = scaled;
+        }
     });
 }
 

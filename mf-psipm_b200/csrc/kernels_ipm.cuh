@@ -426,3 +426,194 @@ __global__ void k_lag_ratio(long long n, const double* __restrict__ w, const dou
 }
 
 }  // namespace psipm
+
+namespace psipm {
+
+// ---- starting point (psipm_active_pool.py:4122-4304, legacy projection) -------
+// Each kernel writes kStartSlots partial results per block into
+// part[slot * gridDim.x + block]; the host folds them in block order, so the
+// starting point is the same on every run.
+constexpr int kStartSlots = 6;
+
+__device__ __forceinline__ void start_partial_sum(double v, int slot, double* part, double* scratch) {
+    v = block_sum(v, scratch);
+    if (threadIdx.x == 0) part[slot * gridDim.x + blockIdx.x] = v;
+}
+__device__ __forceinline__ double block_max(double v, double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (warp == 0) {
+        s = lane < nw ? scratch[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+        if (lane == 0) scratch[0] = s;
+    }
+    __syncthreads();
+    s = scratch[0];
+    __syncthreads();
+    return s;
+}
+__device__ __forceinline__ void start_partial_max(double v, int slot, double* part, double* scratch) {
+    v = block_max(v, scratch);
+    if (threadIdx.x == 0) part[slot * gridDim.x + blockIdx.x] = v;
+}
+
+// *flag = 1 if dx (n) or dy (m) holds a non-finite entry
+__global__ void k_start_finite(long long n, long long m, const double* __restrict__ dx,
+                               const double* __restrict__ dy, int* __restrict__ flag) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    bool bad = false;
+    if (j < n) bad = !isfinite(dx[j]);
+    if (j < m) bad = bad || !isfinite(dy[j]);
+    if (bad) atomicExch(flag, 1);
+}
+
+// x, y from the two projections: part slot 0 = 1 if x holds a non-finite entry,
+// slot 3 = 1 if y does; then xl = pos ? x : 0, xu = box ? u - x : 0 and the
+// infeasibilities slot 1 = max(0, max_pos -xl), slot 2 = max(0, max_box -xu)   (:4135-4160)
+__global__ void k_start_bounds(long long n, long long m, const double* __restrict__ x, const double* __restrict__ y,
+                               const double* __restrict__ u, const unsigned char* __restrict__ pos,
+                               const unsigned char* __restrict__ box, double* __restrict__ xl,
+                               double* __restrict__ xu, double* __restrict__ part) {
+    __shared__ double scratch[32];
+    double bad = 0.0, ybad = 0.0, il = 0.0, iu = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n || j < m; j += stride) {
+        if (j < m && !isfinite(y[j])) ybad = 1.0;
+        if (j >= n) continue;
+        const double xj = x[j];
+        if (!isfinite(xj)) bad = 1.0;
+        const double l = pos[j] ? xj : 0.0;
+        const double r = box[j] ? u[j] - xj : 0.0;
+        xl[j] = l;
+        xu[j] = r;
+        if (pos[j]) il = fmax(il, -l);
+        if (box[j]) iu = fmax(iu, -r);
+    }
+    start_partial_max(bad, 0, part, scratch);
+    start_partial_max(il, 1, part, scratch);
+    start_partial_max(iu, 2, part, scratch);
+    start_partial_max(ybad, 3, part, scratch);
+}
+
+// zero x and/or y when they held a non-finite entry (the reference's fallback)
+__global__ void k_start_zero(long long n, double* __restrict__ v) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j < n) v[j] = 0.0;
+}
+
+// r = c - A^T y (aty given): slot 0 = |c|^2, slot 1 = |r|^2
+__global__ void k_start_dual_norms(long long n, const double* __restrict__ c, const double* __restrict__ aty,
+                                   double* __restrict__ r, double* __restrict__ part) {
+    __shared__ double scratch[32];
+    double cc = 0.0, rr = 0.0;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+         j += (long long)gridDim.x * blockDim.x) {
+        const double rj = c[j] - aty[j];
+        r[j] = rj;
+        cc += c[j] * c[j];
+        rr += rj * rj;
+    }
+    start_partial_sum(cc, 0, part, scratch);
+    start_partial_sum(rr, 1, part, scratch);
+}
+
+__global__ void k_start_scale(long long m, double a, double* __restrict__ y) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < m) y[i] *= a;
+}
+
+// xl += xshift1 (pos), xu += xshift1 (box); dual slacks from r (:4166-4199):
+// c = 0: z = 1 on pos, w = 1 on box; else z = r on lower-only, z = r/2 and
+// w = -r/2 on box; slot 0 = max(0, max_pos -z), slot 1 = max(0, max_box -w)
+__global__ void k_start_slacks(long long n, const double* __restrict__ r, double xshift1, int c_zero,
+                               const unsigned char* __restrict__ pos, const unsigned char* __restrict__ box,
+                               double* __restrict__ xl, double* __restrict__ xu, double* __restrict__ z,
+                               double* __restrict__ w, double* __restrict__ part) {
+    __shared__ double scratch[32];
+    double iz = 0.0, iw = 0.0;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+         j += (long long)gridDim.x * blockDim.x) {
+        const bool p = pos[j], b = box[j];
+        if (p) xl[j] += xshift1;
+        if (b) xu[j] += xshift1;
+        double zj = 0.0, wj = 0.0;
+        if (c_zero) {
+            zj = p ? 1.0 : 0.0;
+            wj = b ? 1.0 : 0.0;
+        } else {
+            if (p && !b) zj = r[j];
+            if (b) {
+                zj = 0.5 * r[j];
+                wj = -0.5 * r[j];
+            }
+            if (p) iz = fmax(iz, -zj);
+            if (b) iw = fmax(iw, -wj);
+        }
+        z[j] = zj;
+        w[j] = wj;
+    }
+    start_partial_max(iz, 0, part, scratch);
+    start_partial_max(iw, 1, part, scratch);
+}
+
+// z += zshift1 (pos), w += zshift1 (box) when c != 0, then the sums of :4200-4215:
+// slots 0..5 = sum_pos xl, sum_box xu, sum_pos z, sum_box w, sum_pos xl z, sum_box xu w
+__global__ void k_start_sums(long long n, double zshift1, const unsigned char* __restrict__ pos,
+                             const unsigned char* __restrict__ box, const double* __restrict__ xl,
+                             const double* __restrict__ xu, double* __restrict__ z, double* __restrict__ w,
+                             double* __restrict__ part) {
+    __shared__ double scratch[32];
+    double a[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+         j += (long long)gridDim.x * blockDim.x) {
+        if (pos[j]) {
+            const double zj = z[j] + zshift1;
+            z[j] = zj;
+            a[0] += xl[j];
+            a[2] += zj;
+            a[4] += xl[j] * zj;
+        }
+        if (box[j]) {
+            const double wj = w[j] + zshift1;
+            w[j] = wj;
+            a[1] += xu[j];
+            a[3] += wj;
+            a[5] += xu[j] * wj;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) start_partial_sum(a[k], k, part, scratch);
+}
+
+// final shifts and the primal point (:4216-4240): xl, xu += xshift2; z, w += zshift2;
+// x = max(xl, 1e-12) on lower-only columns; x = clip(u xl / (xl + xu), floors) on box
+__global__ void k_start_final(long long n, double xshift2, double zshift2, const double* __restrict__ u,
+                              const unsigned char* __restrict__ pos, const unsigned char* __restrict__ box,
+                              double* __restrict__ xl, double* __restrict__ xu, double* __restrict__ x,
+                              double* __restrict__ z, double* __restrict__ w) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const bool p = pos[j], b = box[j];
+    double l = xl[j], r = xu[j];
+    if (p) l += xshift2;
+    if (b) r += xshift2;
+    if (p) z[j] += zshift2;
+    if (b) w[j] += zshift2;
+    if (p && !b) x[j] = fmax(l, 1e-12);
+    if (b) {
+        const double d = l + r;
+        const double xb = d > 0.0 ? u[j] * l / d : 0.5 * u[j];
+        double xf, sf;
+        box_floors(u[j], xf, sf);
+        x[j] = fmin(fmax(xb, xf), u[j] - sf);
+    }
+}
+
+}  // namespace psipm

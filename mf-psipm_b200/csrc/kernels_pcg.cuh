@@ -62,14 +62,22 @@ struct SpmvLayout {
 // bit with acquire loads and a short sleep between them.  Without the sleep
 // several hundred leaders spinning on one word keep its L2 slice busy and slow
 // down the memory accesses of the blocks that are still working.  A wait
-// longer than kBarrierPolls polls sets *err and returns, so the kernel always
-// ends; the host clears the word before every launch and reports the flag.
+// longer than `polls` polls sets *err and returns.  Once *err is set every
+// later wait gives up within kBarrierErrCheck polls (the flag is read every
+// kBarrierErrCheck polls, never on the fast path), and the persistent kernels
+// leave their iteration loops when they see the flag, so a timed-out kernel
+// ends after a few more phases instead of waiting out every later barrier.
+// The host clears the word before every launch and reports the flag.
 constexpr unsigned int kBarrierPolls = 1u << 24;
 constexpr unsigned int kBarrierSleepNs = 64;
+constexpr unsigned int kBarrierErrCheck = 16;
 
 struct GridBarrier {
     unsigned int* bar = nullptr;  // [0] arrival word ([1] unused)
     int* err = nullptr;
+    unsigned int polls = kBarrierPolls;  // poll limit of one wait
+
+    __device__ __forceinline__ bool failed() const { return *((volatile const int*)err) != 0; }
 
     __device__ __forceinline__ void sync() const {
         __syncthreads();
@@ -77,13 +85,14 @@ struct GridBarrier {
             const unsigned int add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
             unsigned int old, cur;
             asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(add) : "memory");
-            for (unsigned int polls = 0;; ++polls) {
+            for (unsigned int n = 0;; ++n) {
                 asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
                 if ((cur ^ old) & 0x80000000u) break;
-                if (polls >= kBarrierPolls) {
+                if (n >= polls) {
                     atomicExch(err, 1);
                     break;
                 }
+                if (n % kBarrierErrCheck == kBarrierErrCheck - 1 && failed()) break;
                 __nanosleep(kBarrierSleepNs);
             }
         }
@@ -723,6 +732,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T, P> a) {
         }
     }
     while ((hsd || info > 0) && it < a.maxit) {
+        if (grid.failed()) break;  // a barrier wait timed out: the host reports it
         // q = H p'   (p <- p' inside phase B)
         acc3[0] = acc3[1] = acc3[2] = 0.0;
         lap(3);
@@ -879,8 +889,11 @@ done:
     }
 }
 
-// Grid-barrier cost probe: `count` barriers, nothing else.
-__global__ void k_barrier_probe(int count, long long* out, GridBarrier grid) {
+// Grid-barrier cost probe: `count` barriers, nothing else.  Block
+// `skip_block` (-1: none) returns without arriving, so the other blocks'
+// first wait runs out its poll limit: the timeout path, without a fault.
+__global__ void k_barrier_probe(int count, long long* out, GridBarrier grid, int skip_block) {
+    if ((int)blockIdx.x == skip_block) return;
     const long long t0 = global_ns();
     for (int i = 0; i < count; ++i) grid.sync();
     if (blockIdx.x == 0 && threadIdx.x == 0) *out = global_ns() - t0;

@@ -20,6 +20,12 @@
 //    call writes every scratch entry before reading it, so nothing has to be
 //    cleared, but two calls whose kernels overlap on the GPU (different
 //    streams, no ordering between them) race on the scratch.
+//  * The cached address belongs to the device's current primary context:
+//    calls must not cross a cudaDeviceReset of that device (after one, the
+//    cached address would point into a context that no longer exists).
+//  * A launch error that the caller left pending makes the call return
+//    PSIPM_ERR_CUDA before it launches anything; the pending error is left in
+//    place for the caller (it is read with cudaPeekAtLastError, not cleared).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -87,6 +93,8 @@ extern "C" int psipm_normal_matvec_static(int64_t m, int64_t n, const int32_t* a
         }
         scratch = g_scratch_addr[device];
     }
+    // an earlier, unrelated launch error of the caller: report it, keep it pending
+    if (cudaPeekAtLastError() != cudaSuccess) return PSIPM_ERR_CUDA;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int threads = 256;
     const long long col_blocks = std::min<long long>((n + threads - 1) / threads, 65535);

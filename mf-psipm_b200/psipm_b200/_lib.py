@@ -100,6 +100,7 @@ SIGNATURES = {
     "psipm_scores": (_I32, [_P, _D, _P, _P]),
     "psipm_refresh_core": (_I32, [_P, _I64, _D, _I32, _P, _I64, _P, _P, _P]),
     "psipm_set_core": (_I32, [_P, _P, _I64]),
+    "psipm_tie_info": (_I32, [_P, _P]),
     "psipm_top_k": (_I32, [_P, _P, _I64, _P, _I64, _P, _P]),
     "psipm_factor": (_I32, [_P, _D, _I32, _P, _P]),
     "psipm_apply": (_I32, [_P, _P, _P]),
@@ -114,6 +115,7 @@ SIGNATURES = {
     "psipm_normal_matvec_static": (_I32, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P]),
     "psipm_debug_apply_trace": (_I32, [_P, _P, _P, _P, _I32, _P, _P]),
     "psipm_timer_stop": (_I32, [_P, _P]),
+    "psipm_debug_barrier_timeout": (_I32, [_P, _I32, _I32, _I32, _P]),
     "psipm_debug_levels": (_I32, [_P, _P, _I32, _P]),
     "psipm_ipm_load": (_I32, [_P, _P, _P, _P, _P, _P]),
     "psipm_ipm_put": (_I32, [_P, _I32, _P, _P, _P, _P]),
@@ -123,6 +125,8 @@ SIGNATURES = {
     "psipm_ipm_theta": (_I32, [_P, _D, _D, _D]),
     "psipm_ipm_targets": (_I32, [_P, _I32, _P]),
     "psipm_ipm_newton": (_I32, [_P, _I32, _D, _I32, _I32, _I32, _D, _P, _P, _P, _P, _P]),
+    "psipm_ipm_start_solve": (_I32, [_P, _I32, _D, _I32, _I32, _I32, _D, _P, _P, _P, _P, _P]),
+    "psipm_ipm_start": (_I32, [_P, _I32, _P]),
     "psipm_ipm_steps": (_I32, [_P, _I32, _D, _P]),
     "psipm_ipm_complementarity": (_I32, [_P, _I32, _D, _D, _D, _P]),
     "psipm_ipm_accept": (_I32, [_P, _D]),

@@ -134,6 +134,12 @@ class NormalEquationsDevice:
             mandatory_local.size, ptr(core), ctypes.byref(ncore), ctypes.byref(retained)))
         return core[: ncore.value].copy(), float(retained.value)
 
+    def tie_info(self) -> dict:
+        """Straddling ties of the top-k selections so far (psipm_tie_info)."""
+        out = np.zeros(4, dtype=np.int64)
+        self._check(self.lib.psipm_tie_info(self.h, ptr(out)))
+        return dict(straddles=int(out[0]), tied=int(out[1]), slots=int(out[2]), selections=int(out[3]))
+
     def set_core(self, core: np.ndarray) -> None:
         core = i64(core)
         self._check(self.lib.psipm_set_core(self.h, ptr(core), core.size))
@@ -256,6 +262,27 @@ class NormalEquationsDevice:
                                               int(replacement), float(gap_tolerance), ptr(alphas), ptr(betas),
                                               ptr(history), ctypes.byref(finite), ctypes.byref(info)))
         return bool(finite.value), self._result(None, info, alphas, betas, history, None)
+
+    def ipm_start_solve(self, which: int, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100,
+                        gap_tolerance=0.1):
+        """One projection of the starting point (which 0: x = A^T dy for r2 = b;
+        1: y = dy for r2 = A c) into the iterate; returns (finite, result)."""
+        alphas = np.empty(max(1, maxit))
+        betas = np.empty(max(1, maxit))
+        history = np.empty(maxit + 2)
+        finite = ctypes.c_int32()
+        info = _lib.PcgInfo()
+        self._check(self.lib.psipm_ipm_start_solve(self.h, int(which), float(tol), int(maxit), int(variant),
+                                                   int(replacement), float(gap_tolerance), ptr(alphas),
+                                                   ptr(betas), ptr(history), ctypes.byref(finite),
+                                                   ctypes.byref(info)))
+        return bool(finite.value), self._result(None, info, alphas, betas, history, None)
+
+    def ipm_start(self, solved: bool) -> np.ndarray:
+        """The rest of the starting point on the device (psipm_ipm_start)."""
+        out = np.zeros(5)
+        self._check(self.lib.psipm_ipm_start(self.h, int(bool(solved)), ptr(out)))
+        return out
 
     def ipm_steps(self, with_corrector: bool = False, gamma: float = 0.0) -> Tuple[float, float]:
         out = np.empty(2)

@@ -1,32 +1,81 @@
 """PS-IPM with the iterate resident in device memory.
 
-Same algorithm, branches and constants as :mod:`psipm_b200.ipm` (the
-reference's ``psipm_solve`` / ``prox_eval``, psipm_active_pool.py:2277-2788
-and :1947-2271), but x, y, z, w, s, the residuals, the complementarity
-targets and the Newton directions never leave the device: every O(n)
+The reference's outer loop (``psipm_solve`` / ``prox_eval``,
+psipm_active_pool.py:2277-2788 and :1947-2271) keeps x, y, z, w, s, the
+residuals and the directions in NumPy and calls the KKT solver across the
+``factorize`` / ``solve`` boundary.  This driver takes the same decisions
+with the same constants, but the vectors never leave the device: every O(n)
 operation is one of the ``psipm_ipm_*`` kernels of the C ABI, and the host
 only sees the scalars the loop branches on (step lengths, trial mu, residual
 norms, outer KKT measures).  The KKT policy object is the same
-``GpuSpectralStableColumnPreconditioner``; it receives ``RESIDENT`` instead of
-a theta array and solves with ``solve_resident``.
+``GpuSpectralStableColumnPreconditioner``; it receives ``RESIDENT`` instead
+of a theta array and solves with ``solve_resident``.
 
-The starting point (psipm_active_pool.py:4122-4304) runs once on the host
-(:func:`psipm_b200.ipm.starting_point`) and is then copied to the device.
+The starting point (psipm_active_pool.py:4122-4304, the default legacy
+projection) runs on the device as well: the policy factors theta = 1, the two
+projections go straight into the device iterate (``solve_start``) and
+``psipm_ipm_start`` forms the shifted start there.
 
-Sums on the device combine block partials in no fixed order, so the
-trajectory matches the host loop to rounding, not bit for bit.
+Sums that the loop branches on are folded from block partials; the
+preconditioner application adds with atomics, so the trajectory is
+reproducible to rounding, not bit for bit.
 """
 
 from __future__ import annotations
 
 import math
 import time
+from dataclasses import dataclass, field
 from typing import Optional
 
 import numpy as np
 
-from .ipm import EPS, Solution, all_or_idx, starting_point
 from .kkt import RESIDENT, GpuSpectralStableColumnPreconditioner, KKTSolveError
+
+EPS = float(np.finfo(np.float64).eps)
+
+
+@dataclass
+class Solution:
+    """Result of a solve, with the field names of the reference's ``Solution``
+    (psipm_active_pool.py:1875-1941) that this driver fills in."""
+
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    w: np.ndarray
+    status: str = "unknown"
+    obj: float = np.nan
+    outer_iter: int = 0
+    inner_iter: int = 0
+    time: float = 0.0
+    t_fact: float = 0.0
+    t_solve: float = 0.0
+    res_p: float = np.nan
+    res_d: float = np.nan
+    mu: float = np.nan
+    gap: float = np.nan
+    history: list = field(default_factory=list)
+    pcg_iterations: int = 0
+    pcg_max_iterations: int = 0
+    n_fact: int = 0
+    n_solve: int = 0
+
+
+def starting_point_resident(dev, kkt, n: int) -> np.ndarray:
+    """Device starting point: factor theta = 1, delta = 1 through the KKT
+    policy (the reference's ``solver.factorize(ones, 1.0)``), the two
+    projections into the device iterate, then the shifts on the device.  Any
+    failure of the factorisation or a projection starts from x = y = 0, as
+    the reference's legacy start does (psipm_active_pool.py:4182-4187)."""
+    solved = True
+    try:
+        kkt.factorize(np.ones(n), 1.0)
+        kkt.solve_start(0)
+        kkt.solve_start(1)
+    except Exception:
+        solved = False
+    return dev.ipm_start(solved)
 
 
 class _Norms:
@@ -203,17 +252,16 @@ def psipm_solve_resident(lp, kkt_solver, tol=1e-6, maxit=200, inner_maxit=100, p
                          time_limit=np.inf, max_outer: Optional[int] = None) -> Solution:
     """Outer proximal loop (psipm_active_pool.py:2277-2788) on device-resident vectors.
 
-    Arguments and result as :func:`psipm_b200.ipm.psipm_solve`; ``kkt_solver``
-    must be a :class:`GpuSpectralStableColumnPreconditioner`.
+    Arguments as the reference's ``psipm_solve`` with an external KKT solver
+    (``max_outer``, not in the reference, stops after that many outer
+    iterations); ``kkt_solver`` must be a
+    :class:`GpuSpectralStableColumnPreconditioner`.
     """
     if not isinstance(kkt_solver, GpuSpectralStableColumnPreconditioner):
         raise TypeError("the device-resident loop needs a GpuSpectralStableColumnPreconditioner")
     A = lp.A
-    At = A.T.tocsr()
     c, b, u = lp.c, lp.b, lp.u
     m, n = A.shape
-    ipos = all_or_idx(lp.pos)
-    ibox = all_or_idx(lp.box)
     npos, nbox = int(lp.pos.sum()), int(lp.box.sum())
     npos_box = npos + nbox
     normA = float(abs(A).sum(axis=1).max()) if A.nnz else 1.0
@@ -231,12 +279,11 @@ def psipm_solve_resident(lp, kkt_solver, tol=1e-6, maxit=200, inner_maxit=100, p
     deadline = tic + time_limit
     dev.ipm_load(c, b, u, lp.pos, lp.box)
     solver.resident = True
-    x, y, z, w = starting_point(A, At, b, c, u, lp, ipos, ibox, solver)
-    dev.ipm_put(0, x, y, z, w)
+    starting_point_resident(dev, solver, n)
     dev.ipm_copy(True)  # centre = iterate
-    solver.h2d_bytes += 8 * (2 * n + m) + 2 * n + 8 * (3 * n + m)
+    solver.h2d_bytes += 8 * (2 * n + m) + 2 * n + 8 * n  # c, u, b, masks, theta = 1
     best_mu = np.inf
-    sol = Solution(x=x, y=y, z=z, w=w)
+    sol = Solution(x=None, y=None, z=None, w=None)
     inner_tot = 0
     it = 0
     nrpi = nrdi = mu = gap = np.nan
@@ -291,3 +338,19 @@ def psipm_solve_resident(lp, kkt_solver, tol=1e-6, maxit=200, inner_maxit=100, p
     sol.n_fact = int(getattr(solver, "n_fact", 0))
     sol.n_solve = int(getattr(solver, "n_solve", 0))
     return sol
+
+
+def solve_standard(lp, tol=1e-8, device=0, precision=0, solver_options=None, **kwargs):
+    """Public entry point: build the device KKT solver for ``lp`` and run the
+    PS-IPM on device-resident vectors (the reference's
+    ``solve_standard``, psipm_spectral_preconditioner.py:755-840, with the
+    spectral stable-column preconditioner).  Returns ``(Solution, solver)``;
+    the caller closes the solver."""
+    opts = dict(solver_options or {})
+    solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, device=device,
+                                                   precision=precision, **opts)
+    try:
+        return psipm_solve_resident(lp, solver, tol=tol, **kwargs), solver
+    except Exception:
+        solver.close()
+        raise

@@ -241,6 +241,7 @@ class GpuStableActiveColumnPreconditioner:
         self.last_factor_info = None
         self.device_seconds = 0.0
         self.core_history = []
+        self.tie_straddles = 0
         # device PCG launches: count, iterations, H·p products, k_pcg seconds
         self.pcg_launches = 0
         self.pcg_total_iterations = 0
@@ -310,6 +311,8 @@ class GpuStableActiveColumnPreconditioner:
         self.core_age = 0
         self._initialized = True
         self.core_history.append(core.copy())
+        # selections whose cut fell inside a run of equal scores (index rule decided)
+        self.tie_straddles = self.dev.tie_info()["straddles"]
 
     def _factor_numeric(self, theta, delta) -> None:
         """Assembly + Jacobi scaling + shift ladder on the device (psipm_active_pool.py:839-897)."""
@@ -608,6 +611,19 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
 
         return self._solve_policy(lambda tol: self._pcg_resident(corrector, tol), lambda finite, res: finite,
                                   fallback if self._minres_available() else None)
+
+    def solve_start(self, which: int) -> bool:
+        """``solve(zeros, b)`` (which 0) or ``solve(zeros, A c)`` (which 1) of
+        the starting point (psipm_active_pool.py:4182-4187) on the device: same
+        policy, statistics and ``KKTSolveError`` as :meth:`solve`; the result
+        goes straight into the device iterate (x = A^T dy, or y = dy).
+        Returns whether it is finite."""
+        return self._solve_policy(lambda tol: self._pcg_start(which, tol), lambda finite, res: finite, None)
+
+    def _pcg_start(self, which, tolerance):
+        finite, res = self.dev.ipm_start_solve(which, tolerance, self.cg_maxit, _lib.PCG_SPECTRAL,
+                                               self.residual_replacement, self.residual_gap_tolerance)
+        return finite, self._krylov(res)
 
     def _solve_policy(self, run, finish, fallback=None):
         started = time.perf_counter()

@@ -318,6 +318,16 @@ def starting_point(A, At, b, c, u, lp, ipos, ibox, solver):
     except Exception:
         x = zeros_n.copy()
         y = np.zeros(m)
+    return start_from_projections(At, c, u, lp, ibox, x, y)
+
+
+def start_from_projections(At, c, u, lp, ibox, x, y):
+    """The starting point's arithmetic after the two projections x = A' dy_b and
+    y = dy_c (psipm_active_pool.py:4190-4240)."""
+    n, m = x.size, y.size
+    zeros_n = np.zeros(n)
+    pos, box = lp.pos, lp.box
+    lower_only = pos & ~box
     if not np.isfinite(x).all():
         x = zeros_n.copy()
     if not np.isfinite(y).all():

@@ -1,8 +1,8 @@
 """A CPU stand-in for ``NormalEquationsDevice`` — test infrastructure.
 
 It answers the same method calls with the oracle's NumPy arithmetic, so the
-host-side policy of ``psipm_b200.kkt`` and the IPM loop of
-``psipm_b200.ipm`` can run without a GPU, and it can be told to fail a given
+host-side policy of ``psipm_b200.kkt`` and the device-resident IPM driver
+``psipm_b200.ipm_device`` can run without a GPU, and it can be told to fail a given
 call with a library status code (host-side fault injection: no device is
 involved, nothing is made to fault).
 """
@@ -66,6 +66,9 @@ class FakeDevice:
 
     def set_core(self, core):
         self.core = np.asarray(core, dtype=np.int64).copy()
+
+    def tie_info(self):
+        return dict(straddles=0, tied=0, slots=0, selections=0)
 
     def refresh_core(self, target, retention, stable, mandatory_local):
         self._maybe_fail("refresh_core")
@@ -220,6 +223,28 @@ class FakeDevice:
         self.rd, self.rp = np.zeros(n), np.zeros(m)
         self.rmz, self.rmw = np.zeros(n), np.zeros(n)
         self.wref = None
+
+    def ipm_start_solve(self, which, tol, maxit, variant=_lib.PCG_SPECTRAL, replacement=100, gap_tolerance=0.1):
+        r2 = self.b if which == 0 else self.A @ self.c
+        dx, res = self.solve(np.zeros(self.n), r2, tol, maxit, variant, replacement, gap_tolerance)
+        if which == 0:
+            self.sets[0][0] = self.At @ res.x
+        else:
+            self.sets[0][1] = res.x.copy()
+        return bool(np.isfinite(dx).all() and np.isfinite(res.x).all()), res
+
+    def ipm_start(self, solved):
+        from oracle import ipm as OI
+
+        class _LP:
+            pos, box = self.pos, self.box
+
+        x, y = self.sets[0][0], self.sets[0][1]
+        if not solved:
+            x, y = np.zeros(self.n), np.zeros(self.m)
+        ibox = slice(None) if self.box.all() else np.flatnonzero(self.box)
+        self.sets[0] = list(OI.start_from_projections(self.At, self.c, self.u, _LP, ibox, x.copy(), y.copy()))
+        return np.zeros(5)
 
     def ipm_put(self, which, x, y, z, w):
         self.sets[which] = [np.array(v, dtype=float) for v in (x, y, z, w)]

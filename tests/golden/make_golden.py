@@ -1,9 +1,10 @@
 """Generate the golden fixtures by running the unmodified reference.
 
-Run in a container that has the reference checked out (read-only) at
-``/root/reference`` or at the path given by ``--reference``:
+Run in a container that has the reference checked out (read-only), giving
+its directory with ``--reference`` or the ``PSIPM_REFERENCE`` environment
+variable:
 
-    python tests/golden/make_golden.py [--reference PATH]
+    python tests/golden/make_golden.py --reference PATH [--only NAME]
 
 The reference needs ``sksparse.cholmod`` (CHOLMOD), which is not installed
 in this image; ``tests/golden/cholmod_standin`` provides the same API on top
@@ -38,7 +39,16 @@ INSTANCES = {
     "cover_m200": ("set_cover", dict(m=200, n=10_000, seed=2000)),
     # four dense columns (1,100 entries each): the Woodbury extraction path
     "dense_m1200": ("random_lp_dense", dict(m=1200, n=3600, seed=7)),
+    # the full-size random LP (m = 2,000, n = 6,000, 5 nonzeros per column) with the
+    # reference's default options: m > 1,500, so the stable core path runs as is
+    "random_m2000": ("random_lp", dict(m=2000, n=6000, seed=0)),
 }
+# per-instance option overrides and number of recorded calls
+INSTANCE_OPTIONS = {"random_m2000": {}}
+INSTANCE_KEEP = {"random_m2000": 4}
+# full solves recorded as a summary only (no per-call vectors): the 200 x 250 grid
+# network LP that the benchmark solves (seed 1000), with the reference's defaults
+RESULTS = {"grid_200x250_result": ("grid_network", dict(rows=200, cols=250, seed=1000))}
 # plus hsd_m1600 (make_hsd): the V3.1 HSD preconditioner surface, and
 # hsd_newton_m1600 (make_hsd_newton): the V3.1 reduced HSD Newton system
 # the small instances use the stable core path (the exact-preconditioner
@@ -48,9 +58,11 @@ OPTIONS = dict(full_preconditioner_row_threshold=10)
 
 def main():
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("PSIPM_REFERENCE"))
     parser.add_argument("--only", default=None)
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("give the reference's directory with --reference or PSIPM_REFERENCE")
     sys.path.insert(0, os.path.join(HERE, "cholmod_standin"))
     sys.path.insert(0, args.reference)
     sys.path.insert(0, os.path.join(REPO, "mf-psipm_b200"))
@@ -75,11 +87,13 @@ def main():
             super()._refresh_core(weights, delta, stable, force_backbone)
             self.rec_cores.append(self.core.copy())
 
+        keep = KEEP_CALLS
+
         def factorize(self, theta, delta):
             self._pending_scores = None
             core_before = self.core.copy()
             super().factorize(theta, delta)
-            if len(self.rec_factor) < KEEP_CALLS:
+            if len(self.rec_factor) < self.keep:
                 self.rec_factor.append(dict(
                     theta=np.array(theta), delta=float(delta), core_before=core_before,
                     core=self.core.copy(), scores=(None if self._pending_scores is None
@@ -88,7 +102,7 @@ def main():
 
         def solve(self, r1, r2):
             dx, dy = super().solve(r1, r2)
-            if len(self.rec_solve) < KEEP_CALLS:
+            if len(self.rec_solve) < self.keep:
                 self.rec_solve.append(dict(
                     r1=np.array(r1), r2=np.array(r2), dx=np.array(dx), dy=np.array(dy),
                     theta=np.array(self.theta), delta=float(self.delta), core=self.core.copy(),
@@ -100,10 +114,12 @@ def main():
             continue
         lp0 = getattr(synthetic, family)(**kwargs)
         lp = PS.StandardLP(c=lp0.c, A=lp0.A, b=lp0.b, u=lp0.u, pos=lp0.pos, box=lp0.box)
-        solver = Recording(lp.A, protected=~lp.pos, **OPTIONS)
+        options = INSTANCE_OPTIONS.get(name, OPTIONS)
+        solver = Recording(lp.A, protected=~lp.pos, **options)
+        solver.keep = INSTANCE_KEEP.get(name, KEEP_CALLS)
         sol = PS.psipm_solve(lp, kkt="spectral-stable-pcg", kkt_solver=solver, tol=1e-8, printlevel=0)
         out = dict(
-            family=family, kwargs=repr(kwargs), options=repr(OPTIONS),
+            family=family, kwargs=repr(kwargs), options=repr(options),
             A_data=lp.A.data, A_indices=lp.A.indices, A_indptr=lp.A.indptr,
             A_shape=np.array(lp.A.shape), b=lp.b, c=lp.c, u=lp.u, pos=lp.pos, box=lp.box,
             x=sol.x, y=sol.y, z=sol.z, w=sol.w, obj=sol.obj, status=sol.status,
@@ -129,10 +145,50 @@ def main():
         print(f"{name}: {sol.status} obj {sol.obj!r} pcg {sol.pcg_iterations} "
               f"-> {os.path.getsize(path) / 1e6:.2f} MB")
 
+    for name, (family, kwargs) in RESULTS.items():
+        if args.only == name:  # long (about 40 minutes on 8 cores): only on request
+            make_result(PS, SSP, synthetic, name, family, kwargs)
     if args.only in (None, "hsd_m1600"):
         make_hsd(PS, synthetic)
     if args.only in (None, "hsd_newton_m1600"):
         make_hsd_newton(synthetic)
+
+
+def make_result(PS, SSP, synthetic, name, family, kwargs):
+    """Full reference solve to 1e-8 with default options, kept as a JSON summary:
+    the outcome (status, objective, residuals, iteration counts), the outer
+    iteration history and the per-call PCG counts and core sizes, plus a
+    fingerprint of the generated LP so that a test can check that it solves
+    the same instance."""
+    import json
+    import time
+
+    lp0 = getattr(synthetic, family)(**kwargs)
+    lp = PS.StandardLP(c=lp0.c, A=lp0.A, b=lp0.b, u=lp0.u, pos=lp0.pos, box=lp0.box)
+    solver = SSP.SpectralStableColumnPreconditioner(lp.A, protected=~lp.pos)
+    t0 = time.perf_counter()
+    sol = PS.psipm_solve(lp, kkt="spectral-stable-pcg", kkt_solver=solver, tol=1e-8, printlevel=0)
+    seconds = time.perf_counter() - t0
+    cx = float(lp.c @ sol.x)
+    ibox = np.flatnonzero(lp.box)
+    gap = abs(cx - (float(lp.b @ sol.y) - float(sol.w[ibox] @ lp.u[ibox]))) / (1.0 + abs(cx))
+    out = dict(
+        family=family, kwargs=kwargs, tol=1e-8, status=sol.status, obj=float(sol.obj),
+        res_p=float(sol.res_p), res_d=float(sol.res_d), mu=float(sol.mu), gap=gap,
+        outer_iter=int(sol.outer_iter), inner_iter=int(sol.inner_iter),
+        pcg_iterations=int(sol.pcg_iterations), n_fact=int(solver.n_fact),
+        cg_iterations=[int(v) for v in solver.cg_iterations],
+        core_sizes=[int(v) for v in solver.core_sizes],
+        history=[{k: float(v) for k, v in h.items() if isinstance(v, (int, float))} for h in sol.history],
+        seconds=seconds, cpu_count=os.cpu_count(),
+        fingerprint=dict(shape=list(lp.A.shape), nnz=int(lp.A.nnz), c_sum=float(lp.c.sum()),
+                         b_abs_sum=float(np.abs(lp.b).sum()), u_sum=float(lp.u[ibox].sum())),
+    )
+    path = os.path.join(HERE, f"{name}.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"{name}: {sol.status} obj {sol.obj!r} outer {sol.outer_iter} pcg {sol.pcg_iterations} "
+          f"in {seconds:.0f} s")
 
 
 def make_hsd(PS, synthetic):

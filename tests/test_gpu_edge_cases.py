@@ -113,3 +113,31 @@ def test_hsd_deadline_stops_after_one_iteration(golden):
         assert ok and it > 1
     finally:
         pre.impl.close()
+
+
+def test_grid_barrier_timeout_ends_quickly_and_leaves_the_handle_usable():
+    """A block that never arrives: the other blocks' first wait runs out its
+    (small) poll limit, sets the timeout flag, and every later wait gives up
+    within a few polls, so 200 barriers end in well under a second with
+    PSIPM_ERR_TIMEOUT; the handle then computes a correct product."""
+    import ctypes
+
+    from psipm_b200 import _lib, synthetic
+    from psipm_b200.device import NormalEquationsDevice
+
+    lp = synthetic.random_lp(200, 600, seed=12)
+    m, n = lp.A.shape
+    dev = NormalEquationsDevice(lp.A)
+    try:
+        secs = ctypes.c_double()
+        # no block skipped: every wait ends normally
+        assert dev.lib.psipm_debug_barrier_timeout(dev.h, 50, 1 << 20, -1, ctypes.byref(secs)) == _lib.OK
+        status = dev.lib.psipm_debug_barrier_timeout(dev.h, 200, 4096, 1, ctypes.byref(secs))
+        assert status == _lib.ERR_TIMEOUT
+        assert secs.value < 1.0, f"timed-out barriers took {secs.value:.3f} s"
+        theta = np.exp(np.random.default_rng(3).uniform(-2.0, 2.0, n))
+        dev.set_theta(theta, 1e-6)
+        v = np.random.default_rng(4).standard_normal(m)
+        assert rel(dev.matvec(v), normal_matrix(lp.A, theta, 1e-6) @ v) < 1e-13
+    finally:
+        dev.close()

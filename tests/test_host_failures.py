@@ -12,7 +12,8 @@ import pytest
 
 from _helpers import exact_direction
 from fake_device import FakeDevice
-from psipm_b200 import _lib, ipm, synthetic
+from oracle import ipm
+from psipm_b200 import _lib, synthetic
 from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner, KKTSolveError
 
 OPTS = dict(full_preconditioner_row_threshold=10)

@@ -3,8 +3,8 @@
 ``FakeDevice`` answers the ``psipm_ipm_*`` calls with NumPy arithmetic that
 follows the reference's prox_eval / psipm_solve (psipm_active_pool.py:
 1947-2271, 2277-2788) line by line, so the resident driver must retrace the
-host loop (psipm_b200.ipm, which passes theta, r1, r2, dx, dy across the KKT
-boundary like the reference) iteration for iteration.  Failures are injected
+host loop (the oracle's restatement of the reference's caller, which passes
+theta, r1, r2, dx, dy across the KKT boundary) iteration for iteration.  Failures are injected
 on the host, as in test_host_failures.py.
 """
 
@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 from fake_device import FakeDevice
-from psipm_b200 import _lib, ipm, synthetic
+from oracle import ipm
+from psipm_b200 import _lib, synthetic
 from psipm_b200.ipm_device import psipm_solve_resident
 from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner
 

@@ -79,3 +79,40 @@ def test_static_matvec_rejects_too_many_columns():
     status = lib.psipm_normal_matvec_static(
         2, _lib.STATIC_SCRATCH_MAX + 1, p(i), p(i), p(x), p(i), p(i), p(x), p(x), 0.0, p(x), p(x), None)
     assert status == _lib.ERR_ARGUMENT
+
+
+def test_static_matvec_at_the_column_limit_on_the_null_stream_leaves_inputs_unchanged():
+    """n exactly at the limit (one nonzero per column keeps it small), the NULL
+    stream, and a check that the call writes only y."""
+    import torch
+
+    from psipm_b200 import _lib
+
+    lib = _lib.load()
+    m, n = 64, _lib.STATIC_SCRATCH_MAX
+    rng = np.random.default_rng(5)
+    rows = rng.integers(0, m, n)
+    A = sp.csc_matrix((rng.standard_normal(n), (rows, np.arange(n))), shape=(m, n))
+    theta = np.exp(rng.uniform(-2.0, 2.0, n))
+    delta = 1e-3
+    d = _device_arrays(torch, A, theta)
+    v = rng.standard_normal(m)
+    v_dev = torch.tensor(v, dtype=torch.float64, device="cuda")
+    y_dev = torch.full((m,), float("nan"), dtype=torch.float64, device="cuda")
+    before = {k: t.clone() for k, t in d.items()}
+    v_before = v_dev.clone()
+    torch.cuda.synchronize()
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    for call in range(2):
+        status = lib.psipm_normal_matvec_static(
+            m, n, p(d["at_ptr"]), p(d["at_idx"]), p(d["at_val"]), p(d["a_ptr"]), p(d["a_idx"]),
+            p(d["a_val"]), p(d["w"]), delta, p(v_dev), p(y_dev), None)
+        assert status == _lib.OK, f"call {call}: status {status}"
+        torch.cuda.synchronize()
+        expected = A @ ((A.T @ v) / theta) + delta * v
+        y = y_dev.cpu().numpy()
+        err = np.linalg.norm(y - expected) / np.linalg.norm(expected)
+        assert err <= 1e-13, f"call {call}: relative difference {err:.2e}"
+    for k, t in d.items():
+        assert torch.equal(t, before[k]), f"{k} was modified"
+    assert torch.equal(v_dev, v_before), "v was modified"
