@@ -340,6 +340,52 @@ int64_t psipm_kernel_launches(const psipm_handle* h);
  * [1] preconditioner apply, [2] vector ops; filled only when profiling is on. */
 int psipm_set_profiling(psipm_handle* h, int32_t on);
 
+/* ---- learned active-column selector ---------------------------------------------
+ * No counterpart in the reference code: a 6 -> 64 -> 64 -> 2 perceptron per
+ * candidate column whose first output re-scores the candidates before the
+ * rule's own core refresh (psipm_refresh_core keeps its mandatory, retention
+ * and trimming steps, psipm_stable_preconditioner.py:311-371) and whose second
+ * output, averaged over the candidates, votes for the factor's first shift
+ * index.  Inputs per column: log theta, log nnz, log |a_j|, log mu, previous
+ * core membership and the spectral rule's log score (_scores,
+ * psipm_stable_preconditioner.py:293-309).  Weights are BF16 (uint16 bit
+ * patterns), biases FP32, arithmetic FP32.  Parameter order: W1[64][6],
+ * W2[64][64], W3[2][64] (the PSIPM_MLP_WEIGHTS BF16 values), then b1[64],
+ * b2[64], b3[2] (the PSIPM_MLP_BIASES FP32 values); gradients and the FP32
+ * master copy use the same order over all PSIPM_MLP_PARAMS values. */
+#define PSIPM_MLP_INPUTS 6
+#define PSIPM_MLP_WEIGHTS 4608
+#define PSIPM_MLP_BIASES 130
+#define PSIPM_MLP_PARAMS 4738
+#define PSIPM_MLP_TILE 128
+/* Copy of the handle's current theta[n] (set by psipm_set_theta or
+ * psipm_ipm_theta) to the host. */
+int psipm_get_theta(psipm_handle* h, double* theta);
+/* Features of every candidate for the current weights and core (psipm_scores
+ * must have run): x[ncand][6] (host). */
+int psipm_mlp_features(psipm_handle* h, double mu, float* x);
+/* Replace the handle's scores by the network's (host weights w, biases b);
+ * *shift_vote (may be NULL) receives the mean second output. */
+int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double mu, double* shift_vote);
+/* Device-pointer kernels for training, on `stream`; they allocate nothing.
+ * forward: out[count][2] for x[count][6].
+ * grad: loss = scale * sum_i c0 (out0_i - y0_i)^2 + c1 (out1_i - y1_i)^2 for
+ * targets y[count][2], and its gradient w.r.t. every parameter (weights as
+ * the BF16 values in use) into grad[PSIPM_MLP_PARAMS]; `blocks` blocks of
+ * PSIPM_MLP_TILE threads each write one partial (part[blocks][PSIPM_MLP_PARAMS],
+ * loss_part[blocks]) and the partials are added in block order, so the result
+ * does not depend on scheduling.
+ * adam: one Adam step (bias corrections for step `step` >= 1, decoupled
+ * weight decay `decay` on the weights) on the FP32 master copy, which is then
+ * rounded into w (BF16) and copied into b. */
+int psipm_mlp_forward_dev(int64_t count, const float* x, const uint16_t* w, const float* b, float* out,
+                          void* stream);
+int psipm_mlp_grad_dev(int64_t count, const float* x, const float* y, float c0, float c1, const uint16_t* w,
+                       const float* b, int32_t blocks, float* part, float* loss_part, float scale, float* grad,
+                       float* loss, void* stream);
+int psipm_mlp_adam_dev(float* master, float* m1, float* m2, const float* grad, float lr, float beta1,
+                       float beta2, float eps, int32_t step, float decay, uint16_t* w, float* b, void* stream);
+
 /* ---- allocation-free operator product -------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory (a host framework that owns the whole device pool,

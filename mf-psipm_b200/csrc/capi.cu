@@ -18,6 +18,7 @@
 #include "common.cuh"
 #include "kernels_factor.cuh"
 #include "kernels_ipm.cuh"
+#include "kernels_mlp.cuh"
 #include "kernels_pcg.cuh"
 #include "kernels_select.cuh"
 #include "symbolic.h"
@@ -2526,6 +2527,104 @@ int psipm_ipm_minres(psipm_handle* h, int32_t corrector, double tol, int32_t max
         int bad = 0;
         read_back(h, &bad, I.flag.p, 1);
         *finite = bad ? 0 : 1;
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Learned active-column selector (kernels_mlp.cuh)
+extern "C" {
+
+int psipm_mlp_forward_dev(int64_t count, const float* x, const uint16_t* w, const float* b, float* out,
+                          void* stream) {
+    if (count < 0 || (count && (!x || !out)) || !w || !b) return PSIPM_ERR_ARGUMENT;
+    if (count == 0) return PSIPM_OK;
+    if ((count + 255) / 256 > 0x7fffffffLL) return PSIPM_ERR_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int grid = (int)((count + 255) / 256);
+    k_mlp_forward<<<grid, 256, 0, st>>>(count, x, reinterpret_cast<const __nv_bfloat16*>(w), b, out);
+    return cudaGetLastError() == cudaSuccess ? PSIPM_OK : PSIPM_ERR_CUDA;
+}
+
+int psipm_mlp_grad_dev(int64_t count, const float* x, const float* y, float c0, float c1, const uint16_t* w,
+                       const float* b, int32_t blocks, float* part, float* loss_part, float scale, float* grad,
+                       float* loss, void* stream) {
+    if (count <= 0 || !x || !y || !w || !b || blocks <= 0 || !part || !loss_part || !grad || !loss)
+        return PSIPM_ERR_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpGradSmem) !=
+        cudaSuccess)
+        return PSIPM_ERR_CUDA;
+    k_mlp_grad<<<blocks, kMlpTile, kMlpGradSmem, st>>>(count, x, y, c0, c1,
+                                                       reinterpret_cast<const __nv_bfloat16*>(w), b, part,
+                                                       loss_part);
+    k_mlp_reduce<<<(kMlpParams + 255) / 256, 256, 0, st>>>(blocks, part, loss_part, scale, grad, loss);
+    return cudaGetLastError() == cudaSuccess ? PSIPM_OK : PSIPM_ERR_CUDA;
+}
+
+int psipm_mlp_adam_dev(float* master, float* m1, float* m2, const float* grad, float lr, float beta1, float beta2,
+                       float eps, int32_t step, float decay, uint16_t* w, float* b, void* stream) {
+    if (!master || !m1 || !m2 || !grad || !w || !b || step <= 0) return PSIPM_ERR_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float bc1 = 1.0f - std::pow(beta1, (float)step), bc2 = 1.0f - std::pow(beta2, (float)step);
+    k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, st>>>(master, m1, m2, grad, lr, beta1, beta2, eps, bc1, bc2,
+                                                         decay, reinterpret_cast<__nv_bfloat16*>(w), b);
+    return cudaGetLastError() == cudaSuccess ? PSIPM_OK : PSIPM_ERR_CUDA;
+}
+
+int psipm_get_theta(psipm_handle* h, double* theta) {
+    if (!theta) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_theta, PSIPM_ERR_STATE, "no weights yet");
+        copy_out(h, theta, h->theta.p, h->n);
+    });
+}
+
+int psipm_mlp_features(psipm_handle* h, double mu, float* x) {
+    if (!x) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->scores_valid, PSIPM_ERR_STATE, "features before scores");
+        const int64_t nc = (int64_t)h->cand.size();
+        if (!nc) return;
+        DevBuf<float> xd;
+        xd.reserve(nc * kMlpIn);
+        const unsigned char* flags = (h->core_flags.p && h->core_flags.n >= (size_t)nc) ? h->core_flags.p : nullptr;
+        LAUNCH(h, k_mlp_features<<<blocks_for(nc, 256), 256, 0, h->stream>>>(
+                      nc, h->d_cand.p, h->at_ptr.p, h->at_val.p, h->theta.p, h->scores.p, flags, mu, xd.p));
+        PSIPM_CUDA(cudaMemcpyAsync(x, xd.p, nc * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        PSIPM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double mu, double* shift_vote) {
+    if (!w || !b) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->scores_valid, PSIPM_ERR_STATE, "learned scores before the rule's scores");
+        const int64_t nc = (int64_t)h->cand.size();
+        if (!nc) return;
+        cudaStream_t st = h->stream;
+        DevBuf<float> xd, out, bd;
+        DevBuf<uint16_t> wd;
+        xd.reserve(nc * kMlpIn);
+        out.reserve(nc * kMlpOut);
+        wd.upload(w, kMlpWeights, st);
+        bd.upload(b, kMlpBiases, st);
+        const unsigned char* flags = (h->core_flags.p && h->core_flags.n >= (size_t)nc) ? h->core_flags.p : nullptr;
+        LAUNCH(h, k_mlp_features<<<blocks_for(nc, 256), 256, 0, st>>>(nc, h->d_cand.p, h->at_ptr.p, h->at_val.p,
+                                                                       h->theta.p, h->scores.p, flags, mu, xd.p));
+        const int grid = (int)((nc + 255) / 256);
+        LAUNCH(h, k_mlp_forward<<<grid, 256, 0, st>>>(nc, xd.p, reinterpret_cast<const __nv_bfloat16*>(wd.p), bd.p,
+                                                      out.p));
+        LAUNCH(h, k_mlp_take_scores<<<blocks_for(nc, 256), 256, 0, st>>>(nc, out.p, h->scores.p));
+        std::vector<float> o(2 * nc);
+        PSIPM_CUDA(cudaMemcpyAsync(o.data(), out.p, 2 * nc * sizeof(float), cudaMemcpyDeviceToHost, st));
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        if (shift_vote) {
+            double v = 0.0;
+            for (int64_t c = 0; c < nc; ++c) v += o[2 * c + 1];
+            *shift_vote = v / (double)nc;
+        }
     });
 }
 

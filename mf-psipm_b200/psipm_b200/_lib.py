@@ -29,6 +29,11 @@ ERR_SYMBOLIC = -8
 ERR_UNSUPPORTED = -9
 
 STATIC_SCRATCH_MAX = 1 << 20  # columns, psipm_normal_matvec_static
+MLP_INPUTS = 6
+MLP_WEIGHTS = 4608
+MLP_BIASES = 130
+MLP_PARAMS = 4738
+MLP_TILE = 128
 
 PCG_SPECTRAL = 0
 PCG_HSD = 1
@@ -135,6 +140,14 @@ SIGNATURES = {
     "psipm_lag_reference": (_I32, [_P]),
     "psipm_lag_ratio": (_I32, [_P, _P]),
     "psipm_minres": (_I32, [_P, _P, _P, _D, _I32, _D, _P, _P, _P]),
+    "psipm_get_theta": (_I32, [_P, _P]),
+    "psipm_mlp_features": (_I32, [_P, _D, _P]),
+    "psipm_mlp_scores": (_I32, [_P, _P, _P, _D, _P]),
+    "psipm_mlp_forward_dev": (_I32, [_I64, _P, _P, _P, _P, _P]),
+    "psipm_mlp_grad_dev": (_I32, [_I64, _P, _P, ctypes.c_float, ctypes.c_float, _P, _P, _I32, _P, _P,
+                                  ctypes.c_float, _P, _P, _P]),
+    "psipm_mlp_adam_dev": (_I32, [_P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                  ctypes.c_float, _I32, ctypes.c_float, _P, _P, _P]),
     "psipm_ipm_minres": (_I32, [_P, _I32, _D, _I32, _D, _P, _P]),
 }
 

@@ -134,6 +134,27 @@ class NormalEquationsDevice:
             mandatory_local.size, ptr(core), ctypes.byref(ncore), ctypes.byref(retained)))
         return core[: ncore.value].copy(), float(retained.value)
 
+    def get_theta(self) -> np.ndarray:
+        out = np.empty(self.n)
+        self._check(self.lib.psipm_get_theta(self.h, ptr(out)))
+        return out
+
+    def mlp_features(self, mu: float) -> np.ndarray:
+        """The learned selector's six inputs per candidate (psipm_mlp_features)."""
+        out = np.empty((self.candidates.size, _lib.MLP_INPUTS), dtype=np.float32)
+        self._check(self.lib.psipm_mlp_features(self.h, float(mu), ptr(out)))
+        return out
+
+    def mlp_scores(self, weights_bf16: np.ndarray, biases: np.ndarray, mu: float) -> float:
+        """Replace the handle's scores by the network's; returns the shift vote."""
+        w = np.ascontiguousarray(weights_bf16, dtype=np.uint16)
+        b = np.ascontiguousarray(biases, dtype=np.float32)
+        if w.size != _lib.MLP_WEIGHTS or b.size != _lib.MLP_BIASES:
+            raise ValueError("selector parameters have the wrong size")
+        vote = ctypes.c_double()
+        self._check(self.lib.psipm_mlp_scores(self.h, ptr(w), ptr(b), float(mu), ctypes.byref(vote)))
+        return float(vote.value)
+
     def tie_info(self) -> dict:
         """Straddling ties of the top-k selections so far (psipm_tie_info)."""
         out = np.zeros(4, dtype=np.int64)

@@ -128,7 +128,8 @@ class GpuStableActiveColumnPreconditioner:
                  full_preconditioner_clique_limit=2e8, full_preconditioner_nnz_limit=10_000_000,
                  adaptive_refresh_row_threshold=20_000, order="best", refine=2, refine_tol=1e-10,
                  fail_tol=1e-6, extract_low_rank=True, low_rank_max_columns=8, low_rank_min_nnz=1024,
-                 low_rank_clique_ratio=2.0, device=0, precision=_lib.FP64, dev=None):
+                 low_rank_clique_ratio=2.0, device=0, precision=_lib.FP64, dev=None, selector=None,
+                 selector_patience=2, selector_shift=True):
         if core_factor <= 0.0:
             raise ValueError("core_factor must be positive")
         if max_core_factor < core_factor:
@@ -242,6 +243,22 @@ class GpuStableActiveColumnPreconditioner:
         self.device_seconds = 0.0
         self.core_history = []
         self.tie_straddles = 0
+        # learned selector (no counterpart in the reference): a SelectorModel that
+        # re-scores the candidates before the rule's refresh; a learned core that
+        # turns out poor by the rule's own signals suspends it for
+        # `selector_patience` refreshes (GpuSpectralStableColumnPreconditioner.factorize)
+        self.selector = selector
+        self.selector_patience = max(1, int(selector_patience))
+        self.selector_shift = bool(selector_shift)
+        self._selector_pause = 0
+        self._core_learned = False
+        self._shift_vote = 0.0
+        self.learned_refreshes = 0
+        self.selector_fallbacks = 0
+        self.mu = 1.0
+        self.delta_now = 0.0
+        self.trace_hook = None   # called at each refresh after the rule's scores (training traces)
+        self.factor_hook = None  # called after each factorisation with the shift index used
         # device PCG launches: count, iterations, H·p products, k_pcg seconds
         self.pcg_launches = 0
         self.pcg_total_iterations = 0
@@ -276,6 +293,7 @@ class GpuStableActiveColumnPreconditioner:
         self.dev.close()
 
     def observe(self, x, z, w, s, mu) -> None:  # psipm_stable_preconditioner.py:285-291
+        self.mu = float(mu)
         normalized = max(float(mu), 0.0) / (1.0 + max(float(mu), 0.0))
         self.current_cg_tol = min(self.cg_tol_max, max(self.cg_tol, float(self.forcing_factor * normalized)))
 
@@ -301,6 +319,15 @@ class GpuStableActiveColumnPreconditioner:
             self.core_history.append(self.core.copy())
             return
         self.dev.scores(self.fill_weight, want=False)
+        if self.trace_hook is not None:
+            self.trace_hook(self)
+        learned = self.selector is not None and self._selector_pause == 0
+        if learned:
+            self._shift_vote = self.dev.mlp_scores(self.selector.weights_bf16, self.selector.biases, self.mu)
+            self.learned_refreshes += 1
+        elif self._selector_pause > 0:
+            self._selector_pause -= 1
+        self._core_learned = learned
         target = min(self.core_target, self.candidates.size)
         mandatory_local = np.searchsorted(self.candidates, self.mandatory)
         core, retained = self.dev.refresh_core(target, self.retention, bool(stable and self.core.size),
@@ -320,6 +347,8 @@ class GpuStableActiveColumnPreconditioner:
         start = 0
         if self._shift > 0.0:
             start = max(0, int(np.searchsorted(SHIFTS, self._shift, side="left")) - 1)
+        if self._core_learned and self.selector_shift:  # the network's shift vote
+            start = max(start, min(len(SHIFTS) - 1, int(self._shift_vote + 0.5)))
         try:
             used, info = self.dev.factor(float(delta), start)
         except DeviceError as exc:
@@ -331,6 +360,8 @@ class GpuStableActiveColumnPreconditioner:
             raise KKTSolveError(str(exc)) from exc
         self.stats["not_pd"] += used - start
         self._shift = SHIFTS[used]
+        if self.factor_hook is not None:
+            self.factor_hook(self, used)
         if used > 0:
             self.n_shifted += 1
         self.n_symbolic = int(info.symbolic_analyses)
@@ -344,6 +375,7 @@ class GpuStableActiveColumnPreconditioner:
 
     def factorize(self, theta, delta) -> None:  # psipm_stable_preconditioner.py:397-432
         theta = theta if theta is RESIDENT else np.asarray(theta, dtype=float)
+        self.delta_now = float(delta)
         self._weights = None
         self._upload_weights(theta, delta)
         poor = self._last_cg >= self.refresh_cg
@@ -449,6 +481,7 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         self._rhs_index = 0
 
     def observe(self, x, z, w, s, mu) -> None:  # :252-258
+        self.mu = float(mu)
         normalized = max(float(mu), 0.0) / (1.0 + max(float(mu), 0.0))
         mu_tol = self.forcing_factor * normalized
         self.current_cg_tol = min(self.cg_tol_max, max(self.cg_tol, min(mu_tol, self._ew_tolerance)))
@@ -517,6 +550,7 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
 
     def factorize(self, theta, delta) -> None:  # :420-467
         theta = theta if theta is RESIDENT else np.asarray(theta, dtype=float)
+        self.delta_now = float(delta)
         self._upload_weights(theta, delta)
         spectral_poor = (self._last_condition >= self.condition_limit
                          and self._last_cg >= max(10, int(0.8 * self.refresh_cg)))
@@ -525,6 +559,12 @@ class GpuSpectralStableColumnPreconditioner(GpuStableActiveColumnPreconditioner)
         can_grow = self.core_target < self.max_core_target
         swap_due = poor and not can_grow and self._poor_streak >= self.swap_patience
         refresh = not self._initialized or self.core_age >= self.core_max_age or (poor and can_grow) or swap_due
+        # learned selector fallback: a learned core that the rule's signals call
+        # poor is replaced now by the plain rule, which also keeps the next refreshes
+        if poor and self._core_learned:
+            self.selector_fallbacks += 1
+            self._selector_pause = self.selector_patience
+            refresh = True
         if refresh:
             self._refresh_core(None, delta, stable=bool(self.core.size), force_backbone=swap_due)
             self._poor_streak = 0

@@ -70,6 +70,23 @@ class FakeDevice:
     def tie_info(self):
         return dict(straddles=0, tied=0, slots=0, selections=0)
 
+    def get_theta(self):
+        return self.theta.copy()
+
+    def mlp_features(self, mu):
+        from oracle import mlp as OM
+
+        flags = np.isin(self.candidates, self.core).astype(float)
+        return OM.features(self.A, self.candidates, self.theta, self._scores, flags, mu).astype(np.float32)
+
+    def mlp_scores(self, weights_bf16, biases, mu):
+        from oracle import mlp as OM
+
+        w = (np.asarray(weights_bf16, dtype=np.uint16).astype(np.uint32) << 16).view(np.float32)
+        out = OM.forward(np.concatenate([w, np.asarray(biases, dtype=np.float32)]), self.mlp_features(mu))
+        self._scores = out[:, 0].copy()
+        return float(out[:, 1].mean())
+
     def refresh_core(self, target, retention, stable, mandatory_local):
         self._maybe_fail("refresh_core")
         scores = self._scores

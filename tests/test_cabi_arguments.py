@@ -28,7 +28,8 @@ def lib():
 
 
 def test_null_handle_is_rejected_by_every_entry_point(lib):
-    skip = {"psipm_create", "psipm_normal_matvec_static"}
+    skip = {"psipm_create", "psipm_normal_matvec_static", "psipm_mlp_forward_dev", "psipm_mlp_grad_dev",
+            "psipm_mlp_adam_dev"}
     checked = 0
     for name, (restype, argtypes) in _lib.SIGNATURES.items():
         if name in skip or not argtypes or argtypes[0] is not P:
@@ -114,3 +115,31 @@ def test_create_rejects_a_null_output_and_oversized_problems(lib):
     handle = P()
     assert lib.psipm_create(1 << 31, 1, 0, colptr.ctypes.data, None, None, 0, _lib.FP64,
                             ctypes.byref(handle)) == _lib.ERR_UNSUPPORTED
+
+
+def test_selector_training_kernels_reject_null_arguments(lib):
+    """The device-pointer training entry points check their pointers and sizes
+    before any CUDA call."""
+    buf = (ctypes.c_float * 8)()
+    p = ctypes.cast(buf, P)
+    f = ctypes.c_float
+    assert lib.psipm_mlp_forward_dev(-1, p, p, p, p, None) == _lib.ERR_ARGUMENT
+    assert lib.psipm_mlp_forward_dev(4, None, p, p, p, None) == _lib.ERR_ARGUMENT
+    assert lib.psipm_mlp_forward_dev(0, None, p, p, None, None) == _lib.OK  # nothing to do
+    good = [4, p, p, f(1.0), f(0.0), p, p, 2, p, p, f(1.0), p, p, None]
+    for k in (1, 2, 5, 6, 8, 9, 11, 12):
+        args = list(good)
+        args[k] = None
+        assert lib.psipm_mlp_grad_dev(*args) == _lib.ERR_ARGUMENT, k
+    for k, bad in ((0, 0), (7, 0)):
+        args = list(good)
+        args[k] = bad
+        assert lib.psipm_mlp_grad_dev(*args) == _lib.ERR_ARGUMENT, k
+    adam = [p, p, p, p, f(1e-3), f(0.9), f(0.999), f(1e-8), 1, f(0.0), p, p, None]
+    for k in (0, 1, 2, 3, 10, 11):
+        args = list(adam)
+        args[k] = None
+        assert lib.psipm_mlp_adam_dev(*args) == _lib.ERR_ARGUMENT, k
+    args = list(adam)
+    args[8] = 0
+    assert lib.psipm_mlp_adam_dev(*args) == _lib.ERR_ARGUMENT
