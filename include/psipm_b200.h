@@ -340,6 +340,20 @@ int64_t psipm_kernel_launches(const psipm_handle* h);
  * [1] preconditioner apply, [2] vector ops; filled only when profiling is on. */
 int psipm_set_profiling(psipm_handle* h, int32_t on);
 
+/* ---- HSD pricing over all columns -------------------------------------------------
+ * The pricing round of the V3.1 HSD loop (psipm_v3_1_hsd.py:2101-2158):
+ * violation = A^T y - c tau over every column of the handle's A (products and
+ * sums in index order, no contraction: bit-identical to SciPy's product), the
+ * inactive columns (active[j] == 0) whose violation exceeds `threshold`
+ * (the caller passes pricing_tolerance * max(tau, 1e-12)), and among them
+ * the `batch` largest violations (pricing_batch; the reference's argpartition,
+ * ties by ascending index here).  psipm_price_load stores c[n] once per LP.
+ * candidates (capacity min(n, batch)) receive ascending column indices,
+ * violation[n] (may be NULL) the full vector for the caller's reduced costs. */
+int psipm_price_load(psipm_handle* h, const double* c);
+int psipm_price(psipm_handle* h, const double* y, double tau, const uint8_t* active, double threshold,
+                int64_t batch, double* violation, int64_t* candidates, int64_t* ncandidates);
+
 /* ---- learned active-column selector ---------------------------------------------
  * No counterpart in the reference code: a 6 -> 64 -> 64 -> 2 perceptron per
  * candidate column whose first output re-scores the candidates before the

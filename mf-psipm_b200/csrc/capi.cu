@@ -177,6 +177,10 @@ struct psipm_handle {
     DevBuf<int> eq, eqscan;
     DevBuf<unsigned int> hist;
     DevBuf<unsigned long long> counter;
+    // HSD pricing: costs of all columns and per-round buffers
+    DevBuf<double> price_c, price_y, price_v;
+    DevBuf<unsigned char> price_active, price_elig, price_pick;
+    bool have_price_c = false;
     // straddling ties (keys equal to the selection threshold outnumber the
     // slots left for them): cumulative count, and the last one's sizes
     int64_t tie_straddles = 0, tie_tied = 0, tie_slots = 0, selections = 0;
@@ -2625,6 +2629,48 @@ int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double 
             for (int64_t c = 0; c < nc; ++c) v += o[2 * c + 1];
             *shift_vote = v / (double)nc;
         }
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// HSD pricing over all columns (psipm_v3_1_hsd.py:2101-2158)
+extern "C" {
+
+int psipm_price_load(psipm_handle* h, const double* c) {
+    if (!c) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        h->price_c.upload(c, h->n, h->stream);
+        h->have_price_c = true;
+    });
+}
+
+int psipm_price(psipm_handle* h, const double* y, double tau, const uint8_t* active, double threshold,
+                int64_t batch, double* violation, int64_t* candidates, int64_t* ncandidates) {
+    if (!y || !active || batch < 0 || !candidates || !ncandidates) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->have_price_c, PSIPM_ERR_STATE, "pricing before psipm_price_load");
+        const int64_t n = h->n;
+        cudaStream_t st = h->stream;
+        h->price_y.upload(y, h->m, st);
+        h->price_active.upload(active, n, st);
+        h->price_v.reserve(std::max<int64_t>(1, n));
+        h->price_elig.reserve(std::max<int64_t>(1, n));
+        h->price_pick.zero(std::max<int64_t>(1, n), st);
+        if (n)
+            LAUNCH(h, k_price<<<blocks_for(n, 256), 256, 0, st>>>(n, h->at_ptr.p, h->at_idx.p, h->at_val.p,
+                                                                   h->price_y.p, h->price_c.p, tau,
+                                                                   h->price_active.p, threshold, h->price_v.p,
+                                                                   h->price_elig.p));
+        // eligible columns, the `batch` largest violations among them (index rule on ties)
+        select_top(h, h->price_v.p, h->price_elig.p, n, batch, h->price_pick.p);
+        std::vector<unsigned char> pick = download_flags(h, h->price_pick.p, n);
+        int64_t k = 0;
+        for (int64_t j = 0; j < n; ++j)
+            if (pick[j]) candidates[k++] = j;
+        *ncandidates = k;
+        copy_out(h, violation, h->price_v.p, n);
     });
 }
 

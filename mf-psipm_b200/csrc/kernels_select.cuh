@@ -193,4 +193,21 @@ __global__ void k_flag_op(long long n, const unsigned char* __restrict__ a,
     out[i] = op == 0 ? (unsigned char)(a[i] && !b[i]) : (unsigned char)(a[i] || b[i]);
 }
 
+// ---- HSD pricing (psipm_v3_1_hsd.py:2101-2158) ---------------------------------
+// violation_j = (A^T y)_j - c_j tau, with the products and sums in index order
+// and no contraction (bit-identical to SciPy's CSR product); eligible_j = 1 for
+// inactive columns with violation_j > threshold
+__global__ void k_price(long long n, const int* __restrict__ at_ptr, const int* __restrict__ at_idx,
+                        const double* __restrict__ at_val, const double* __restrict__ y,
+                        const double* __restrict__ c, double tau, const unsigned char* __restrict__ active,
+                        double threshold, double* __restrict__ violation, unsigned char* __restrict__ eligible) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double s = 0.0;
+    for (int k = at_ptr[j]; k < at_ptr[j + 1]; ++k) s = __dadd_rn(s, __dmul_rn(at_val[k], y[at_idx[k]]));
+    const double v = __dsub_rn(s, __dmul_rn(c[j], tau));
+    violation[j] = v;
+    eligible[j] = (unsigned char)(!active[j] && v > threshold);
+}
+
 }  // namespace psipm

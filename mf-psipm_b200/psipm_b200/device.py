@@ -134,6 +134,25 @@ class NormalEquationsDevice:
             mandatory_local.size, ptr(core), ctypes.byref(ncore), ctypes.byref(retained)))
         return core[: ncore.value].copy(), float(retained.value)
 
+    def price_load(self, c: np.ndarray) -> None:
+        c = f64(c)
+        if c.shape != (self.n,):
+            raise ValueError("c has the wrong dimension")
+        self._check(self.lib.psipm_price_load(self.h, ptr(c)))
+
+    def price(self, y, tau: float, active: np.ndarray, threshold: float, batch: int):
+        """HSD pricing round (psipm_price): returns (violation, candidates)."""
+        y = f64(y)
+        act = np.ascontiguousarray(active, dtype=np.uint8)
+        if y.shape != (self.m,) or act.shape != (self.n,):
+            raise ValueError("y or the active mask has the wrong dimension")
+        violation = np.empty(self.n)
+        cand = np.empty(max(1, min(self.n, int(batch))), dtype=np.int64)
+        count = ctypes.c_int64()
+        self._check(self.lib.psipm_price(self.h, ptr(y), float(tau), ptr(act), float(threshold), int(batch),
+                                         ptr(violation), ptr(cand), ctypes.byref(count)))
+        return violation, cand[: count.value].copy()
+
     def get_theta(self) -> np.ndarray:
         out = np.empty(self.n)
         self._check(self.lib.psipm_get_theta(self.h, ptr(out)))

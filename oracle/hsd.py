@@ -222,3 +222,19 @@ class HSDNewtonSystemOracle:
         dkappa = (rhs_t - st.kappa * dtau) / st.tau
         finite = all(np.all(np.isfinite(a)) for a in (dx, dy, dz, dw, np.asarray([dtau, dtheta, dkappa])))
         return dx, dy, dz, dw, float(dtau), float(dtheta), float(dkappa), bool(ok_u and ok_h and ok_t and finite)
+
+
+def pricing_round(A, c, y, tau, active, pricing_tolerance, pricing_batch):
+    """The pricing step of the V3.1 HSD loop (psipm_v3_1_hsd.py:2101-2103,
+    2148-2156): violation over all columns and the candidate columns, ties at
+    the batch cut taken by ascending index (the reference's argpartition
+    leaves that choice to NumPy's build)."""
+    import numpy as np
+
+    tau_scale = max(tau, 1.0e-12)
+    violation = A.T.tocsr() @ y - c * tau
+    candidate = np.flatnonzero(~np.asarray(active, dtype=bool) & (violation > pricing_tolerance * tau_scale))
+    if candidate.size > pricing_batch:
+        order = np.lexsort((candidate, -violation[candidate]))
+        candidate = np.sort(candidate[order[:pricing_batch]])
+    return violation, candidate
