@@ -340,6 +340,23 @@ int64_t psipm_kernel_launches(const psipm_handle* h);
  * [1] preconditioner apply, [2] vector ops; filled only when profiling is on. */
 int psipm_set_profiling(psipm_handle* h, int32_t on);
 
+/* ---- network tree-plus-diagonal preconditioner ------------------------------------
+ * The V3.1 TreePreconditioner (psipm_v3_1_hsd.py:715-785) for incidence
+ * matrices (exactly two entries per column): psipm_set_tree installs the
+ * spanning forest of NetworkTopology.from_incidence (:495-610) -- parent[m]
+ * (-1 at roots), depth[m], and per column the child end of a forest arc or -1
+ * (tree_child[n]) -- and switches the handle from the supernodal factor to
+ * the tree (FP64 handles only; psipm_factor then refuses).
+ * psipm_tree_factor(weights = D[n], delta) forms the pivots and multipliers
+ * level by level (:732-760); every later apply and PCG of the handle uses the
+ * tree solve (:762-776).  Factor and solve perform the reference's operations
+ * in its order, so their results are bit-identical.  psipm_tree_get copies
+ * pivot[m] and multiplier[m] (either may be NULL) to the host.  The PCG's
+ * operator still uses the weights of psipm_set_theta. */
+int psipm_set_tree(psipm_handle* h, const int32_t* parent, const int32_t* depth, const int32_t* tree_child);
+int psipm_tree_factor(psipm_handle* h, const double* weights, double delta);
+int psipm_tree_get(psipm_handle* h, double* pivot, double* multiplier);
+
 /* ---- HSD pricing over all columns -------------------------------------------------
  * The pricing round of the V3.1 HSD loop (psipm_v3_1_hsd.py:2101-2158):
  * violation = A^T y - c tau over every column of the handle's A (products and

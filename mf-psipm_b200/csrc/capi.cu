@@ -177,6 +177,13 @@ struct psipm_handle {
     DevBuf<int> eq, eqscan;
     DevBuf<unsigned int> hist;
     DevBuf<unsigned long long> counter;
+    // network tree-plus-diagonal preconditioner (psipm_set_tree / psipm_tree_factor)
+    bool tree_mode = false, tree_ready = false;
+    int tree_levels = 0;
+    DevBuf<int> t_level_ptr, t_level_nodes, t_parent, t_kid_ptr, t_kids, t_fptr, t_fcol, t_sptr, t_scol, t_cptr,
+        t_ccol;
+    DevBuf<double> t_D, t_diag, t_tw, t_piv, t_mult, t_pivot, t_val;
+    std::vector<int> t_level_ptr_host, t_level_nodes_host;
     // HSD pricing: costs of all columns and per-round buffers
     DevBuf<double> price_c, price_y, price_v;
     DevBuf<unsigned char> price_active, price_elig, price_pick;
@@ -404,6 +411,19 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
             pc.lr_chol = h->lr_chol.p;
             pc.lr_part = h->lr_part.p;
         }
+    }
+    if (h->tree_ready) {
+        TreeLayout& t = pc.tree;
+        t.m = (int)h->m;
+        t.nlevels = h->tree_levels;
+        t.level_ptr = h->t_level_ptr.p;
+        t.level_nodes = h->t_level_nodes.p;
+        t.parent = h->t_parent.p;
+        t.kid_ptr = h->t_kid_ptr.p;
+        t.kids = h->t_kids.p;
+        t.mult = h->t_mult.p;
+        t.pivot = h->t_pivot.p;
+        t.val = h->t_val.p;
     }
     PcgStore<T>& st = pstore(h, tag);
     const int64_t m = h->m, n = h->n;
@@ -1318,6 +1338,7 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
     if (start_shift < 0 || start_shift > 7) return PSIPM_ERR_ARGUMENT;
     int status = guarded(h, [&]() {
         require(h->have_theta, PSIPM_ERR_STATE, "factor before set_theta");
+        require(!h->tree_mode, PSIPM_ERR_STATE, "the handle uses the tree preconditioner (psipm_tree_factor)");
         if (h->core_dirty || !h->have_symbolic) analyse(h);
         h->delta = delta;
         Symbolic& s = h->sym;
@@ -2671,6 +2692,127 @@ int psipm_price(psipm_handle* h, const double* y, double tau, const uint8_t* act
             if (pick[j]) candidates[k++] = j;
         *ncandidates = k;
         copy_out(h, violation, h->price_v.p, n);
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Network tree-plus-diagonal preconditioner (psipm_v3_1_hsd.py:715-785)
+extern "C" {
+
+int psipm_set_tree(psipm_handle* h, const int32_t* parent, const int32_t* depth, const int32_t* tree_child) {
+    if (!parent || !depth || !tree_child) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        const int64_t m = h->m, n = h->n;
+        require(h->precision == PSIPM_FP64, PSIPM_ERR_UNSUPPORTED, "the tree preconditioner is FP64 only");
+        int maxd = 0;
+        for (int64_t i = 0; i < m; ++i) {
+            require(depth[i] >= 0 && depth[i] < m, PSIPM_ERR_ARGUMENT, "depth out of range");
+            require(parent[i] >= -1 && parent[i] < m, PSIPM_ERR_ARGUMENT, "parent out of range");
+            require((parent[i] < 0) == (depth[i] == 0), PSIPM_ERR_ARGUMENT, "roots are the nodes at depth 0");
+            if (parent[i] >= 0)
+                require(depth[parent[i]] == depth[i] - 1, PSIPM_ERR_ARGUMENT, "a parent is one level up");
+            maxd = std::max(maxd, (int)depth[i]);
+        }
+        // every column: exactly two entries; its first and second row
+        std::vector<int> first(n), second(n);
+        for (int64_t j = 0; j < n; ++j) {
+            require(h->colptr[j + 1] - h->colptr[j] == 2, PSIPM_ERR_ARGUMENT,
+                    "the tree preconditioner needs exactly two entries per column");
+            first[j] = h->rowidx[h->colptr[j]];
+            second[j] = h->rowidx[h->colptr[j] + 1];
+            const int c = tree_child[j];
+            require(c == -1 || ((c == first[j] || c == second[j]) && parent[c] == (c == first[j] ? second[j] : first[j])),
+                    PSIPM_ERR_ARGUMENT, "tree_child must name the arc's child end in the forest");
+        }
+        const int L = maxd + 1;
+        // nodes by level (ascending within a level), children lists, arc lists
+        std::vector<int> lptr(L + 1, 0), lnodes(m), kptr(m + 1, 0), kids;
+        for (int64_t i = 0; i < m; ++i) ++lptr[depth[i] + 1];
+        for (int l = 0; l < L; ++l) lptr[l + 1] += lptr[l];
+        {
+            std::vector<int> f(lptr.begin(), lptr.end() - 1);
+            for (int64_t i = 0; i < m; ++i) lnodes[f[depth[i]]++] = (int)i;
+        }
+        for (int64_t i = 0; i < m; ++i)
+            if (parent[i] >= 0) ++kptr[parent[i] + 1];
+        for (int64_t i = 0; i < m; ++i) kptr[i + 1] += kptr[i];
+        kids.resize(kptr[m]);
+        {
+            std::vector<int> f(kptr.begin(), kptr.end() - 1);
+            for (int64_t i = 0; i < m; ++i)
+                if (parent[i] >= 0) kids[f[parent[i]]++] = (int)i;
+        }
+        auto lists = [&](const std::vector<int>& key, std::vector<int>& ptr, std::vector<int>& col) {
+            ptr.assign(m + 1, 0);
+            for (int64_t j = 0; j < n; ++j)
+                if (key[j] >= 0) ++ptr[key[j] + 1];
+            for (int64_t i = 0; i < m; ++i) ptr[i + 1] += ptr[i];
+            col.resize(ptr[m]);
+            std::vector<int> f(ptr.begin(), ptr.end() - 1);
+            for (int64_t j = 0; j < n; ++j)
+                if (key[j] >= 0) col[f[key[j]]++] = (int)j;
+        };
+        std::vector<int> fptr, fcol, sptr, scol, cptr, ccol, tc(tree_child, tree_child + n);
+        lists(first, fptr, fcol);
+        lists(second, sptr, scol);
+        lists(tc, cptr, ccol);
+        cudaStream_t st = h->stream;
+        h->t_level_ptr.upload(lptr, st);
+        h->t_level_nodes.upload(lnodes, st);
+        std::vector<int> par(parent, parent + m);
+        h->t_parent.upload(par, st);
+        h->t_kid_ptr.upload(kptr, st);
+        h->t_kids.upload(kids.empty() ? std::vector<int>{0} : kids, st);
+        h->t_fptr.upload(fptr, st);
+        h->t_fcol.upload(fcol, st);
+        h->t_sptr.upload(sptr, st);
+        h->t_scol.upload(scol, st);
+        h->t_cptr.upload(cptr, st);
+        h->t_ccol.upload(ccol.empty() ? std::vector<int>{0} : ccol, st);
+        for (DevBuf<double>* v : {&h->t_diag, &h->t_tw, &h->t_piv, &h->t_mult, &h->t_pivot, &h->t_val})
+            v->reserve(std::max<int64_t>(1, m));
+        h->t_D.reserve(std::max<int64_t>(1, n));
+        h->t_level_ptr_host = lptr;
+        h->t_level_nodes_host = lnodes;
+        h->tree_levels = L;
+        h->tree_mode = true;
+        h->tree_ready = false;
+        h->have_factor = false;
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int psipm_tree_factor(psipm_handle* h, const double* weights, double delta) {
+    if (!weights) return PSIPM_ERR_ARGUMENT;
+    return guarded(h, [&]() {
+        require(h->tree_mode, PSIPM_ERR_STATE, "tree factor before psipm_set_tree");
+        const int m = (int)h->m;
+        cudaStream_t st = h->stream;
+        h->t_D.upload(weights, h->n, st);
+        LAUNCH(h, k_tree_diag<<<blocks_for(m, 256), 256, 0, st>>>(m, delta, h->t_fptr.p, h->t_fcol.p, h->t_sptr.p,
+                                                                   h->t_scol.p, h->t_cptr.p, h->t_ccol.p, h->t_D.p,
+                                                                   h->t_diag.p, h->t_tw.p));
+        for (int l = h->tree_levels - 1; l >= 0; --l) {
+            const int beg = h->t_level_ptr_host[l], cnt = h->t_level_ptr_host[l + 1] - beg;
+            if (cnt)
+                LAUNCH(h, k_tree_pivots<<<blocks_for(cnt, 256), 256, 0, st>>>(
+                              cnt, h->t_level_nodes.p + beg, l > 0, h->t_kid_ptr.p, h->t_kids.p, h->t_diag.p,
+                              h->t_tw.p, h->t_piv.p, h->t_mult.p));
+        }
+        const double floor = std::max(delta * 1.0e-8, 2.2250738585072014e-308);
+        LAUNCH(h, k_tree_floor<<<blocks_for(m, 256), 256, 0, st>>>(m, floor, h->t_piv.p, h->t_pivot.p));
+        h->tree_ready = true;
+        h->have_factor = true;
+    });
+}
+
+int psipm_tree_get(psipm_handle* h, double* pivot, double* multiplier) {
+    return guarded(h, [&]() {
+        require(h->tree_ready, PSIPM_ERR_STATE, "no tree factor");
+        copy_out(h, pivot, h->t_pivot.p, h->m);
+        copy_out(h, multiplier, h->t_mult.p, h->m);
     });
 }
 

@@ -20,6 +20,7 @@
 #include <cooperative_groups.h>
 
 #include "common.cuh"
+#include "kernels_tree.cuh"
 
 namespace psipm {
 
@@ -154,6 +155,9 @@ struct PrecLayout {
     const double* lr_B = nullptr;     // P_base^{-1} A_L, m x q column-major
     const double* lr_chol = nullptr;  // Cholesky factor of the q x q core, row-major lower
     double* lr_part = nullptr;        // per-block partial sums, gridDim.x x kLowRankMax
+    // network tree-plus-diagonal preconditioner instead of the supernodal factor
+    // (tree.nlevels > 0; FP64 handles only)
+    TreeLayout tree;
 };
 
 template <typename T, typename P = T>
@@ -553,11 +557,53 @@ __device__ void prec_low_rank(const PrecLayout<P>& pc, const IT* in, IT* out, do
     }
 }
 
+// Tree-plus-diagonal solve (kernels_tree.cuh) over the whole grid: one grid
+// barrier per level and direction; the same operations in the same order as
+// the reference's TreePreconditioner.solve (psipm_v3_1_hsd.py:764-776).
+template <typename IT>
+__device__ void prec_tree(const TreeLayout& t, const IT* in, IT* out, double& acc_rz, const GridBarrier& grid) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gstride = gridDim.x * blockDim.x;
+    double* v = t.val;
+    for (int i = gtid; i < t.m; i += gstride) v[i] = (double)in[i];
+    grid.sync();
+    for (int l = t.nlevels - 2; l >= 0; --l) {  // parents at level l gather their children
+        for (int q = t.level_ptr[l] + gtid; q < t.level_ptr[l + 1]; q += gstride) {
+            const int p = t.level_nodes[q];
+            double a = v[p];
+            for (int k = t.kid_ptr[p]; k < t.kid_ptr[p + 1]; ++k) {
+                const int c = t.kids[k];
+                a = __dadd_rn(a, __dmul_rn(-t.mult[c], v[c]));
+            }
+            v[p] = a;
+        }
+        grid.sync();
+    }
+    for (int i = gtid; i < t.m; i += gstride) v[i] = __ddiv_rn(v[i], t.pivot[i]);
+    grid.sync();
+    for (int l = 1; l < t.nlevels; ++l) {
+        for (int q = t.level_ptr[l] + gtid; q < t.level_ptr[l + 1]; q += gstride) {
+            const int c = t.level_nodes[q];
+            v[c] = __dsub_rn(v[c], __dmul_rn(t.mult[c], v[t.parent[c]]));
+        }
+        grid.sync();
+    }
+    for (int i = gtid; i < t.m; i += gstride) {
+        const IT zi = (IT)v[i];
+        out[i] = zi;
+        acc_rz += (double)in[i] * (double)zi;
+    }
+}
+
 // z = P^{-1} in; acc_rz += in . z.  Ends without a barrier (the caller's
 // reduction provides it).
 template <typename P, typename IT>
 __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, double& acc_rz, P* fs,
                            const GridBarrier& grid) {
+    if (pc.tree.nlevels > 0) {
+        prec_tree(pc.tree, in, out, acc_rz, grid);
+        return;
+    }
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;

@@ -141,6 +141,9 @@ SIGNATURES = {
     "psipm_lag_ratio": (_I32, [_P, _P]),
     "psipm_minres": (_I32, [_P, _P, _P, _D, _I32, _D, _P, _P, _P]),
     "psipm_get_theta": (_I32, [_P, _P]),
+    "psipm_set_tree": (_I32, [_P, _P, _P, _P]),
+    "psipm_tree_factor": (_I32, [_P, _P, _D]),
+    "psipm_tree_get": (_I32, [_P, _P, _P]),
     "psipm_price_load": (_I32, [_P, _P]),
     "psipm_price": (_I32, [_P, _P, _D, _P, _D, _I64, _P, _P, _P]),
     "psipm_mlp_features": (_I32, [_P, _D, _P]),

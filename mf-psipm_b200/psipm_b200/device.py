@@ -134,6 +134,25 @@ class NormalEquationsDevice:
             mandatory_local.size, ptr(core), ctypes.byref(ncore), ctypes.byref(retained)))
         return core[: ncore.value].copy(), float(retained.value)
 
+    def set_tree(self, parent, depth, tree_child) -> None:
+        """Switch to the network tree-plus-diagonal preconditioner (psipm_set_tree)."""
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+        parent, depth, tree_child = i32(parent), i32(depth), i32(tree_child)
+        if parent.shape != (self.m,) or depth.shape != (self.m,) or tree_child.shape != (self.n,):
+            raise ValueError("forest arrays have the wrong dimensions")
+        self._check(self.lib.psipm_set_tree(self.h, ptr(parent), ptr(depth), ptr(tree_child)))
+
+    def tree_factor(self, weights, delta: float) -> None:
+        w = f64(weights)
+        if w.shape != (self.n,):
+            raise ValueError("weights have the wrong dimension")
+        self._check(self.lib.psipm_tree_factor(self.h, ptr(w), float(delta)))
+
+    def tree_get(self):
+        pivot, mult = np.empty(self.m), np.empty(self.m)
+        self._check(self.lib.psipm_tree_get(self.h, ptr(pivot), ptr(mult)))
+        return pivot, mult
+
     def price_load(self, c: np.ndarray) -> None:
         c = f64(c)
         if c.shape != (self.n,):

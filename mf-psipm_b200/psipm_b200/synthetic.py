@@ -143,8 +143,11 @@ def _ground(A: sp.csc_matrix) -> np.ndarray:
     return np.flatnonzero(keep)
 
 
-def grid_network(rows: int = 200, cols: int = 250, long_range: float = 0.10, seed: int = 1000) -> StandardLP:
-    """Grounded min-cost flow LP on a directed grid plus random long-range arcs."""
+def grid_network(rows: int = 200, cols: int = 250, long_range: float = 0.10, seed: int = 1000,
+                 ground: bool = True) -> StandardLP:
+    """Grounded min-cost flow LP on a directed grid plus random long-range arcs
+    (``ground=False`` keeps every node row: a pure incidence matrix, the case
+    of the reference's network preconditioner)."""
     rng = np.random.default_rng(seed)
     nodes = rows * cols
     idx = np.arange(nodes).reshape(rows, cols)
@@ -166,7 +169,7 @@ def grid_network(rows: int = 200, cols: int = 250, long_range: float = 0.10, see
     cap = rng.integers(10, 1001, narcs).astype(np.float64)
     flow = np.floor(rng.random(narcs) * (cap + 1.0))
     b_full = A_full @ flow
-    keep = _ground(A_full)
+    keep = _ground(A_full) if ground else np.arange(nodes)
     A = A_full[keep, :]
     b = b_full[keep]
     return _finish(A, b, cost, cap, f"grid_network_{rows}x{cols}_s{seed}",

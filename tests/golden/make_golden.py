@@ -148,6 +148,8 @@ def main():
     for name, (family, kwargs) in RESULTS.items():
         if args.only == name:  # long (about 40 minutes on 8 cores): only on request
             make_result(PS, SSP, synthetic, name, family, kwargs)
+    if args.only in (None, "tree_grid_20x25"):
+        make_tree(synthetic)
     if args.only in (None, "hsd_m1600"):
         make_hsd(PS, synthetic)
     if args.only in (None, "hsd_newton_m1600"):
@@ -189,6 +191,48 @@ def make_result(PS, SSP, synthetic, name, family, kwargs):
         json.dump(out, f, indent=1)
     print(f"{name}: {sol.status} obj {sol.obj!r} outer {sol.outer_iter} pcg {sol.pcg_iterations} "
           f"in {seconds:.0f} s")
+
+
+def make_tree(synthetic):
+    """V3.1 network surface: NetworkTopology.from_incidence and TreePreconditioner
+    (psipm_v3_1_hsd.py:495-610, 715-785) on an ungrounded 20 x 25 grid network,
+    with a random active-column set containing the protected forest arcs:
+    the forest, then three factorisations (random weights, delta) each with
+    two solves, and the HSD _pcg (:1015-1063) with the tree as preconditioner."""
+    import psipm_v3_1_hsd as H
+
+    lp = synthetic.grid_network(20, 25, seed=1001, ground=False)
+    A = lp.A.tocsc()
+    topo = H.NetworkTopology.from_incidence(A)
+    rng = np.random.default_rng(23)
+    active = np.flatnonzero(topo.protected | (rng.random(A.shape[1]) < 0.6))
+    pre = H.TreePreconditioner(topo, active)
+    out = dict(A_data=A.data, A_indices=A.indices, A_indptr=A.indptr, A_shape=np.array(A.shape),
+               parent=topo.parent, depth=topo.depth, tree_child=topo.tree_child, protected=topo.protected,
+               root=topo.root, components=topo.components, active=active)
+    Aa = A[:, active]
+    for call in range(3):
+        D = np.exp(rng.uniform(-6.0, 6.0, active.size))
+        delta = float(10.0 ** rng.uniform(-10, -4))
+        pre.factor(D, delta)
+        out.update({f"c{call}_D": D, f"c{call}_delta": delta, f"c{call}_pivot": pre.pivot.copy(),
+                    f"c{call}_multiplier": pre.multiplier.copy()})
+        for k in range(2):
+            rhs = rng.standard_normal(A.shape[0])
+            out[f"c{call}_rhs{k}"] = rhs
+            out[f"c{call}_sol{k}"] = pre.solve(rhs)
+
+        def matvec(v, D=D, delta=delta):
+            return Aa @ (D * (Aa.T @ v)) + delta * v
+
+        rhs = Aa @ (D * rng.standard_normal(active.size))
+        x, it, mv, ok, _ = H._pcg(matvec, rhs, pre, 1e-10, 1000, np.inf)
+        out.update({f"c{call}_pcg_rhs": rhs, f"c{call}_pcg_x": x, f"c{call}_pcg_iterations": it,
+                    f"c{call}_pcg_ok": ok})
+    path = os.path.join(HERE, "tree_grid_20x25.npz")
+    np.savez_compressed(path, **out)
+    print(f"tree_grid_20x25: depth {int(topo.depth.max())}, active {active.size}, PCG "
+          f"{[int(out[f'c{i}_pcg_iterations']) for i in range(3)]} -> {os.path.getsize(path) / 1e6:.2f} MB")
 
 
 def make_hsd(PS, synthetic):
