@@ -3,8 +3,9 @@
 * Random LP, m = 2,000, n = 6,000 (fixture ``random_m2000``, written by the
   unmodified reference with its default options): per call, scores
   bit-identical, refreshed cores identical, the device Newton direction
-  within 1e-6 relative of the reference's own FP64 PCG direction at the
-  reference's tolerance, with the same PCG iteration count up to one; the
+  (with the reference's lagged factor where it reused one) within 1e-6
+  relative of the reference's own FP64 PCG direction at the reference's
+  tolerance, with the same PCG iteration count up to one; the
   complete device PS-IPM solve optimal at the reference's objective to 1e-8.
 * Grid min-cost-flow LP, 200 x 250 (the benchmark's LP, seed 1000): the
   complete device-resident solve optimal, objective within 1e-8 relative of
@@ -52,11 +53,17 @@ def test_random_m2000_per_call_parity(golden):
             assert np.array_equal(core, g[f"f{i}_core"]), f"core, call {i}"
             scored += 1
         assert scored
+        nf = int(g["n_factor_calls"])
         for i in range(int(g["n_solve_calls"])):
             theta, delta, tol = g[f"s{i}_theta"], float(g[f"s{i}_delta"]), float(g[f"s{i}_tolerance"])
-            dev.set_theta(theta, delta)
+            # the preconditioner of this solve: the factor of the last factorize call that
+            # refactored (factor_age 0) -- a lagged factor keeps an older theta
+            k = max(j for j in range(nf) if np.array_equal(g[f"f{j}_theta"], theta))
+            k = max(j for j in range(k + 1) if int(g[f"f{j}_factor_age"]) == 0)
             dev.set_core(g[f"s{i}_core"])
-            dev.factor(delta, 0)
+            dev.set_theta(g[f"f{k}_theta"], float(g[f"f{k}_delta"]))
+            dev.factor(float(g[f"f{k}_delta"]), 0)
+            dev.set_theta(theta, delta)  # the operator's weights; the factor stays
             dx, res = dev.solve(g[f"s{i}_r1"], g[f"s{i}_r2"], tol, 200, 0, 100, 0.1)
             err_y, err_x = rel(res.x, g[f"s{i}_dy"]), rel(dx, g[f"s{i}_dx"])
             print(f"call {i}: tol {tol:.0e}, iterations {res.iterations} (reference "
