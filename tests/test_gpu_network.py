@@ -1,14 +1,14 @@
 """The network tree-plus-diagonal preconditioner on the device against the
 reference's fixture ``tree_grid_20x25`` (psipm_v3_1_hsd.py:715-785):
 pivots, multipliers and solves bit-identical; the HSD PCG with the tree as
-preconditioner converges and its solution agrees with a direct solve (1e-7
-relative) and with the reference's PCG solution; a rebuilt HSD Newton solve
-through GpuTreePreconditioner.solve_normal returns the exact direction."""
+preconditioner reaches its residual bound in the reference's iteration count
+(within two) and agrees with the reference's PCG solution (1e-7 relative); an
+HSD Newton solve through GpuTreePreconditioner.solve_normal meets its residual
+bound and returns dx = D (r1 + A' dy)."""
 
 import numpy as np
 import pytest
 import scipy.sparse as sp
-import scipy.sparse.linalg as spla
 
 from _helpers import rel
 
@@ -40,17 +40,20 @@ def test_tree_factor_solve_and_pcg_match_the_reference(golden):
             rhs = g[f"c{c}_pcg_rhs"]
             res = pre.dev.pcg(rhs, 1e-10, 1000, _lib.PCG_HSD)
             H = (Aa @ sp.diags(D) @ Aa.T + delta * sp.eye(A.shape[0])).tocsc()
-            exact = spla.spsolve(H, rhs)
+            # an ungrounded incidence matrix: H is singular up to delta, so the
+            # check is the residual the PCG promises, not the distance to a direct solve
+            resid = np.linalg.norm(rhs - H @ res.x) / np.linalg.norm(rhs)
             print(f"call {c}: PCG {res.iterations} iterations (reference {int(g[f'c{c}_pcg_iterations'])}), "
-                  f"error vs direct {rel(res.x, exact):.2e}, vs reference {rel(res.x, g[f'c{c}_pcg_x']):.2e}")
+                  f"relative residual {resid:.2e}, difference from the reference {rel(res.x, g[f'c{c}_pcg_x']):.2e}")
             assert res.ok and bool(g[f"c{c}_pcg_ok"])
-            assert rel(res.x, exact) <= 1e-7
+            assert resid <= 1.01e-10
+            assert abs(res.iterations - int(g[f"c{c}_pcg_iterations"])) <= 2
             assert rel(res.x, g[f"c{c}_pcg_x"]) <= 1e-7
             r1 = np.random.default_rng(c).standard_normal(active.size)
             r2 = np.random.default_rng(c + 7).standard_normal(A.shape[0])
             dx, dy, it, mv, ok, _ = pre.solve_normal(r1, r2, 1e-12, 2000)
-            dy_e = spla.spsolve(H, r2 - Aa @ (D * r1))
-            assert ok and rel(dy, dy_e) <= 1e-7
-            assert rel(dx, D * (r1 + Aa.T @ dy_e)) <= 1e-7
+            rhs2 = r2 - Aa @ (D * r1)
+            assert ok and np.linalg.norm(rhs2 - H @ dy) <= 1.01e-12 * np.linalg.norm(rhs2)
+            assert rel(dx, D * (r1 + Aa.T @ dy)) <= 1e-12
     finally:
         pre.close()
