@@ -97,7 +97,7 @@ struct psipm_handle {
     DevBuf<double> at_val, a_val;
     DevBuf<int> short_rows, long_rows, long_chunk_ptr, chunk_beg, chunk_end, chunk_row;
     int64_t short_nnz = 0;
-    int n_short = 0, n_long = 0, n_chunks = 0, vw = 32, cw = 1;
+    int n_short = 0, n_long = 0, n_chunks = 0, vw = 32;
     long long pcg_budget_ns = 0;  // psipm_set_pcg_budget (0: none)
     DevBuf<long long> d_cand;
 
@@ -295,14 +295,6 @@ void build_matrix(psipm_handle* h) {
     int vw = 1;
     while (vw < 32 && vw < avg) vw <<= 1;
     h->vw = vw;
-    // lanes per column of the A^T products: the power of two at or below the
-    // mean column length (2 for incidence columns, 4 for 5-entry columns)
-    {
-        const double mean_col = n ? (double)nnz / (double)n : 1.0;
-        int cw = 1;
-        while (cw < 32 && 2 * cw <= mean_col) cw <<= 1;
-        h->cw = cw;
-    }
     h->n_short = (int)shortr.size();
     h->n_long = (int)longr.size();
     h->n_chunks = (int)cb.size();
@@ -331,7 +323,6 @@ SpmvLayout spmv_layout(psipm_handle* h) {
     s.a_ptr = h->a_ptr.p;
     s.a_idx = h->a_idx.p;
     s.vw = h->vw;
-    s.cw = h->cw;
     s.short_rows = h->short_rows.p;
     s.n_short = h->n_short;
     s.long_rows = h->long_rows.p;

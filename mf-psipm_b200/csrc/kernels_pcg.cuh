@@ -45,7 +45,6 @@ struct SpmvLayout {
     const int* a_ptr = nullptr;   // A in CSR: m rows
     const int* a_idx = nullptr;
     int vw = 32;                  // lanes per short row (power of two)
-    int cw = 1;                   // lanes per column in A^T products (power of two)
     const int* short_rows = nullptr;
     int n_short = 0;
     const int* long_rows = nullptr;
@@ -226,65 +225,27 @@ __device__ __forceinline__ void read_totals(const double* part, double (&tot)[K]
 // ---- phase A: t = w o (A^T src) -----------------------------------------
 // src: 0 -> v, 1 -> z, 2 -> z + beta p
 template <typename T, typename P>
-__device__ __forceinline__ T src_value(const PcgArgs<T, P>& a, const T* v, int src, T beta, int i) {
-    return src == 0 ? v[i] : (src == 1 ? a.z[i] : a.z[i] + beta * a.p[i]);
-}
-
-// A sub-warp of cw lanes per column (cw a power of two near the mean column
-// length; cw = 1 is a thread per column).  Each lane loads its strided entries
-// of the column at once (no chain of dependent loads through the column), and
-// the lanes' sums meet in a butterfly, a fixed order.
-template <typename T, typename P>
 __device__ void phase_a(const PcgArgs<T, P>& a, const T* v, int src, T beta) {
-    const int lane = threadIdx.x & 31;
-    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int cw = a.sp.cw;
-    const int per_warp = 32 / cw;
-    const int sub = lane / cw, sl = lane % cw;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gstride = gridDim.x * blockDim.x;
     const int* __restrict__ ptr = a.sp.at_ptr;
     const int* __restrict__ idx = a.sp.at_idx;
     const T* __restrict__ val = a.at_val;
-    for (int base = gwarp * per_warp; base < a.sp.n; base += nwarps * per_warp) {
-        const int j = base + sub;
-        const bool valid = j < a.sp.n;
+    for (int j = gtid; j < a.sp.n; j += gstride) {
+        const int b = ptr[j], e = ptr[j + 1];
         T s = 0;
-        if (valid) {
-            const int b = ptr[j], e = ptr[j + 1];
-            for (int k = b + sl; k < e; k += cw) s += val[k] * src_value(a, v, src, beta, idx[k]);
+        if (src == 0) {
+            for (int k = b; k < e; ++k) s += val[k] * v[idx[k]];
+        } else if (src == 1) {
+            for (int k = b; k < e; ++k) s += val[k] * a.z[idx[k]];
+        } else {
+            for (int k = b; k < e; ++k) {
+                const int i = idx[k];
+                s += val[k] * (a.z[i] + beta * a.p[i]);
+            }
         }
-        for (int o = cw >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (valid && sl == 0) a.t[j] = a.w[j] * s;
+        a.t[j] = a.w[j] * s;
     }
-}
-
-// Strided partial sum s += val[k] * t[idx[k]] for k = k0, k0 + stride, ... < e,
-// in that order, with the loads of kBatch entries issued before their
-// products are added (more loads in flight, the same additions in the same
-// order as a plain loop).
-constexpr int kBatch = 4;
-template <typename T>
-__device__ __forceinline__ T strided_dot(const T* __restrict__ val, const int* __restrict__ idx, const T* t, int k0,
-                                         int e, int stride) {
-    T s = 0;
-    for (int k = k0; k < e; k += kBatch * stride) {
-        int ii[kBatch];
-        T vv[kBatch];
-#pragma unroll
-        for (int q = 0; q < kBatch; ++q) {
-            const int kk = k + q * stride;
-            const int kc = kk < e ? kk : k;
-            ii[q] = idx[kc];
-            vv[q] = val[kc];
-        }
-        T tt[kBatch];
-#pragma unroll
-        for (int q = 0; q < kBatch; ++q) tt[q] = t[ii[q]];
-#pragma unroll
-        for (int q = 0; q < kBatch; ++q)
-            if (k + q * stride < e) s += vv[q] * tt[q];
-    }
-    return s;
 }
 
 // ---- phase B: rows of A t, with an epilogue per mode -----------------------
@@ -332,13 +293,17 @@ __device__ void phase_b(const PcgArgs<T, P>& a, int mode, int src, T beta, doubl
         const bool valid = ri < a.sp.n_short;
         const int i = valid ? a.sp.short_rows[ri] : 0;
         T s = 0;
-        if (valid) s = strided_dot(val, idx, t, ptr[i] + sl, ptr[i + 1], vw);
+        if (valid) {
+            const int b = ptr[i], e = ptr[i + 1];
+            for (int k = b + sl; k < e; k += vw) s += val[k] * t[idx[k]];
+        }
         for (int o = vw >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (valid && sl == 0) row_epilogue(a, mode, src, beta, i, s, acc);
     }
     // long rows: chunk partial sums (finished in phase_b2)
     for (int c = gwarp; c < a.sp.n_chunks; c += nwarps) {
-        T s = strided_dot(val, idx, t, a.sp.chunk_beg[c] + lane, a.sp.chunk_end[c], 32);
+        T s = 0;
+        for (int k = a.sp.chunk_beg[c] + lane; k < a.sp.chunk_end[c]; k += 32) s += val[k] * t[idx[k]];
         s = warp_sum(s);
         if (lane == 0) a.chunk_part[c] = s;
     }

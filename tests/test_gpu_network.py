@@ -51,9 +51,9 @@ def test_tree_factor_solve_and_pcg_match_the_reference(golden):
             assert rel(res.x, g[f"c{c}_pcg_x"]) <= 1e-7
             r1 = np.random.default_rng(c).standard_normal(active.size)
             r2 = np.random.default_rng(c + 7).standard_normal(A.shape[0])
-            dx, dy, it, mv, ok, _ = pre.solve_normal(r1, r2, 1e-12, 2000)
+            dx, dy, it, mv, ok, _ = pre.solve_normal(r1, r2, 1e-9, 2000)
             rhs2 = r2 - Aa @ (D * r1)
-            assert ok and np.linalg.norm(rhs2 - H @ dy) <= 1.01e-12 * np.linalg.norm(rhs2)
+            assert ok and np.linalg.norm(rhs2 - H @ dy) <= 1.01e-9 * np.linalg.norm(rhs2)
             assert rel(dx, D * (r1 + Aa.T @ dy)) <= 1e-12
     finally:
         pre.close()
