@@ -396,8 +396,11 @@ int psipm_get_theta(psipm_handle* h, double* theta);
  * must have run): x[ncand][6] (host). */
 int psipm_mlp_features(psipm_handle* h, double mu, float* x);
 /* Replace the handle's scores by the network's (host weights w, biases b);
+ * with keep > 0 only the rule's `keep` best candidates (by the scores in
+ * place) keep a score, the others become -inf and no selection takes them.
  * *shift_vote (may be NULL) receives the mean second output. */
-int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double mu, double* shift_vote);
+int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double mu, int64_t keep,
+                     double* shift_vote);
 /* Device-pointer kernels for training, on `stream`; they allocate nothing.
  * forward: out[count][2] for x[count][6].
  * grad: loss = scale * sum_i c0 (out0_i - y0_i)^2 + c1 (out1_i - y1_i)^2 for

@@ -2622,7 +2622,8 @@ int psipm_mlp_features(psipm_handle* h, double mu, float* x) {
     });
 }
 
-int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double mu, double* shift_vote) {
+int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double mu, int64_t keep,
+                     double* shift_vote) {
     if (!w || !b) return PSIPM_ERR_ARGUMENT;
     return guarded(h, [&]() {
         require(h->scores_valid, PSIPM_ERR_STATE, "learned scores before the rule's scores");
@@ -2641,7 +2642,16 @@ int psipm_mlp_scores(psipm_handle* h, const uint16_t* w, const float* b, double 
         const int grid = (int)((nc + 255) / 256);
         LAUNCH(h, k_mlp_forward<<<grid, 256, 0, st>>>(nc, xd.p, reinterpret_cast<const __nv_bfloat16*>(wd.p), bd.p,
                                                       out.p));
-        LAUNCH(h, k_mlp_take_scores<<<blocks_for(nc, 256), 256, 0, st>>>(nc, out.p, h->scores.p));
+        // keep > 0: only the rule's `keep` best candidates stay eligible (the others
+        // become -inf, which no selection takes); the network orders them
+        const unsigned char* allow = nullptr;
+        DevBuf<unsigned char> top;
+        if (keep > 0 && keep < nc) {
+            top.zero(nc, st);
+            select_top(h, h->scores.p, nullptr, nc, keep, top.p);
+            allow = top.p;
+        }
+        LAUNCH(h, k_mlp_take_scores<<<blocks_for(nc, 256), 256, 0, st>>>(nc, out.p, allow, h->scores.p));
         std::vector<float> o(2 * nc);
         PSIPM_CUDA(cudaMemcpyAsync(o.data(), out.p, 2 * nc * sizeof(float), cudaMemcpyDeviceToHost, st));
         PSIPM_CUDA(cudaStreamSynchronize(st));

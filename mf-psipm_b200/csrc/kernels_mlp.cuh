@@ -299,10 +299,11 @@ __global__ void k_mlp_features(long long ncand, const long long* __restrict__ ca
     o[5] = (float)(0.1 * log(fmax(score[c], 1e-300)));
 }
 
-// scores (FP64, candidate order) = out[:, 0]
-__global__ void k_mlp_take_scores(long long ncand, const float* __restrict__ out, double* __restrict__ score) {
+// scores (FP64, candidate order) = out[:, 0]; where allow (may be null) is 0: -inf
+__global__ void k_mlp_take_scores(long long ncand, const float* __restrict__ out,
+                                  const unsigned char* __restrict__ allow, double* __restrict__ score) {
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (c < ncand) score[c] = (double)out[2 * c];
+    if (c < ncand) score[c] = (allow && !allow[c]) ? -INFINITY : (double)out[2 * c];
 }
 
 }  // namespace psipm

@@ -147,7 +147,7 @@ SIGNATURES = {
     "psipm_price_load": (_I32, [_P, _P]),
     "psipm_price": (_I32, [_P, _P, _D, _P, _D, _I64, _P, _P, _P]),
     "psipm_mlp_features": (_I32, [_P, _D, _P]),
-    "psipm_mlp_scores": (_I32, [_P, _P, _P, _D, _P]),
+    "psipm_mlp_scores": (_I32, [_P, _P, _P, _D, _I64, _P]),
     "psipm_mlp_forward_dev": (_I32, [_I64, _P, _P, _P, _P, _P]),
     "psipm_mlp_grad_dev": (_I32, [_I64, _P, _P, ctypes.c_float, ctypes.c_float, _P, _P, _I32, _P, _P,
                                   ctypes.c_float, _P, _P, _P]),

@@ -183,14 +183,15 @@ class NormalEquationsDevice:
         self._check(self.lib.psipm_mlp_features(self.h, float(mu), ptr(out)))
         return out
 
-    def mlp_scores(self, weights_bf16: np.ndarray, biases: np.ndarray, mu: float) -> float:
-        """Replace the handle's scores by the network's; returns the shift vote."""
+    def mlp_scores(self, weights_bf16: np.ndarray, biases: np.ndarray, mu: float, keep: int = 0) -> float:
+        """Replace the handle's scores by the network's (only the rule's `keep`
+        best candidates stay eligible when keep > 0); returns the shift vote."""
         w = np.ascontiguousarray(weights_bf16, dtype=np.uint16)
         b = np.ascontiguousarray(biases, dtype=np.float32)
         if w.size != _lib.MLP_WEIGHTS or b.size != _lib.MLP_BIASES:
             raise ValueError("selector parameters have the wrong size")
         vote = ctypes.c_double()
-        self._check(self.lib.psipm_mlp_scores(self.h, ptr(w), ptr(b), float(mu), ctypes.byref(vote)))
+        self._check(self.lib.psipm_mlp_scores(self.h, ptr(w), ptr(b), float(mu), int(keep), ctypes.byref(vote)))
         return float(vote.value)
 
     def tie_info(self) -> dict:

@@ -129,7 +129,7 @@ class GpuStableActiveColumnPreconditioner:
                  adaptive_refresh_row_threshold=20_000, order="best", refine=2, refine_tol=1e-10,
                  fail_tol=1e-6, extract_low_rank=True, low_rank_max_columns=8, low_rank_min_nnz=1024,
                  low_rank_clique_ratio=2.0, device=0, precision=_lib.FP64, dev=None, selector=None,
-                 selector_patience=2, selector_shift=True):
+                 selector_patience=2, selector_shift=True, selector_window=0.0):
         if core_factor <= 0.0:
             raise ValueError("core_factor must be positive")
         if max_core_factor < core_factor:
@@ -250,6 +250,8 @@ class GpuStableActiveColumnPreconditioner:
         self.selector = selector
         self.selector_patience = max(1, int(selector_patience))
         self.selector_shift = bool(selector_shift)
+        # > 1: the network only reorders the rule's best selector_window x target candidates
+        self.selector_window = float(selector_window)
         self._selector_pause = 0
         self._core_learned = False
         self._shift_vote = 0.0
@@ -323,7 +325,9 @@ class GpuStableActiveColumnPreconditioner:
             self.trace_hook(self)
         learned = self.selector is not None and self._selector_pause == 0
         if learned:
-            self._shift_vote = self.dev.mlp_scores(self.selector.weights_bf16, self.selector.biases, self.mu)
+            keep = (int(np.ceil(self.selector_window * min(self.core_target, self.candidates.size)))
+                    if self.selector_window > 1.0 else 0)
+            self._shift_vote = self.dev.mlp_scores(self.selector.weights_bf16, self.selector.biases, self.mu, keep)
             self.learned_refreshes += 1
         elif self._selector_pause > 0:
             self._selector_pause -= 1

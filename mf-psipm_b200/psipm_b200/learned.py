@@ -258,26 +258,33 @@ def collect_traces(lp, samples_per_refresh: int = 20000, probes: int = 48, seed:
 
 
 def train_selector(traces: List[Trace], epochs: int = 12, seed: int = 0, device: int = 0, lr: float = 2e-3,
-                   batch: int = 65536) -> Dict:
-    """Train a fresh model on the pooled traces; returns the model and the loss history."""
+                   batch: int = 65536, target: str = "linear") -> Dict:
+    """Train a fresh model on the pooled traces; returns the model and the loss
+    history.  target "linear" regresses the true leverage itself, "log" its
+    logarithm (floored at 1e-4), which weighs the ordering of small leverages
+    as much as that of large ones."""
     x = np.concatenate([t.features for t in traces])
-    y = np.concatenate([t.targets for t in traces])
+    y = np.concatenate([t.targets for t in traces]).copy()
+    if target == "log":
+        y[:, 0] = np.log(np.maximum(y[:, 0], 1e-4))
     model = SelectorModel(seed=seed)
     trainer = DeviceTrainer(model, device=device, lr=lr)
     history = trainer.fit(x, y, epochs=epochs, batch=batch, seed=seed)
     return dict(model=model, history=history, samples=int(x.shape[0]))
 
 
-def compare(lp, model: SelectorModel, tol: float = 1e-8, device: int = 0, solver_options=None) -> Dict:
+def compare(lp, model: SelectorModel, tol: float = 1e-8, device: int = 0, solver_options=None,
+            windows=(0.0,)) -> Dict:
     """Solve `lp` with the plain rule and with the selector (plus its fallback),
     both device-resident; returns time, PCG iterations and outcome of each."""
     from .ipm_device import psipm_solve_resident
     from .kkt import GpuSpectralStableColumnPreconditioner
 
     out = {}
-    for name, sel in (("rule", None), ("learned", model)):
+    arms = [("rule", None, 0.0)] + [("learned" if w <= 1.0 else f"learned_window{w:g}", model, w) for w in windows]
+    for name, sel, window in arms:
         solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, device=device, selector=sel,
-                                                       **(solver_options or {}))
+                                                       selector_window=window, **(solver_options or {}))
         try:
             solver.dev.timer_start()
             sol = psipm_solve_resident(lp, solver, tol=tol)
@@ -309,7 +316,22 @@ def main(argv=None) -> None:
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--out", required=True)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--model", default=None, help="evaluate this model instead of training one")
+    ap.add_argument("--windows", default="0", help="comma-separated selector windows to compare")
+    ap.add_argument("--target", default="linear", choices=("linear", "log"))
     args = ap.parse_args(argv)
+    windows = tuple(float(w) for w in args.windows.split(","))
+    if args.model:
+        model = SelectorModel.load(args.model)
+        report = dict(model=args.model, held_out={})
+        for s in _seeds(args.test):
+            lp = synthetic.grid_network(args.rows, args.cols, seed=1500 + s)
+            report["held_out"][s] = compare(lp, model, windows=windows)
+            print(f"held-out seed {s}: {report['held_out'][s]}", flush=True)
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(report, f, indent=1)
+        return
     t0 = time.time()
     traces = []
     for s in _seeds(args.train):
@@ -317,15 +339,15 @@ def main(argv=None) -> None:
         traces.append(collect_traces(lp, samples_per_refresh=args.samples, probes=args.probes, seed=s))
         print(f"trace seed {s}: {traces[-1].refreshes} refreshes, {traces[-1].features.shape[0]} samples, "
               f"solve {traces[-1].solve}", flush=True)
-    result = train_selector(traces, epochs=args.epochs)
+    result = train_selector(traces, epochs=args.epochs, target=args.target)
     print(f"trained on {result['samples']} samples, loss by epoch {result['history']}", flush=True)
     result["model"].save(args.out, rows=args.rows, cols=args.cols, train=args.train, samples=result["samples"],
-                         history=result["history"])
+                         history=result["history"], target=args.target, probes=args.probes)
     report = dict(train=args.train, samples=result["samples"], history=result["history"], held_out={},
                   trace_seconds=time.time() - t0)
     for s in _seeds(args.test):
         lp = synthetic.grid_network(args.rows, args.cols, seed=1500 + s)
-        report["held_out"][s] = compare(lp, result["model"])
+        report["held_out"][s] = compare(lp, result["model"], windows=windows)
         print(f"held-out seed {s}: {report['held_out'][s]}", flush=True)
     if args.report:
         with open(args.report, "w") as f:

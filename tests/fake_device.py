@@ -79,12 +79,17 @@ class FakeDevice:
         flags = np.isin(self.candidates, self.core).astype(float)
         return OM.features(self.A, self.candidates, self.theta, self._scores, flags, mu).astype(np.float32)
 
-    def mlp_scores(self, weights_bf16, biases, mu):
+    def mlp_scores(self, weights_bf16, biases, mu, keep=0):
         from oracle import mlp as OM
 
         w = (np.asarray(weights_bf16, dtype=np.uint16).astype(np.uint32) << 16).view(np.float32)
         out = OM.forward(np.concatenate([w, np.asarray(biases, dtype=np.float32)]), self.mlp_features(mu))
-        self._scores = out[:, 0].copy()
+        scores = out[:, 0].copy()
+        if 0 < keep < scores.size:
+            allowed = np.zeros(scores.size, dtype=bool)
+            allowed[OS.top_k(self._scores, keep)] = True
+            scores[~allowed] = -np.inf
+        self._scores = scores
         return float(out[:, 1].mean())
 
     def refresh_core(self, target, retention, stable, mandatory_local):
