@@ -18,6 +18,10 @@ Keys of the JSON line:
 * roofline   the persistent PCG kernel (k_pcg): algorithmic bytes of all
              its launches / its CUDA-event time, against the measured HBM
              copy bandwidth;
+* learned_selector  the same solve with the learned active-column selector
+             (psipm_b200.learned, trained on solver traces of other seeds of
+             this LP family) over --selector-steps solves; `value` stays the
+             plain spectral rule;
 * cpu_baseline  the CPU oracle (reference algorithm, SuperLU stand-in
              factor) timed on a bounded sample of the same LP (its first K
              outer iterations), next to the device's time for the same K
@@ -72,6 +76,11 @@ def parse():
     ap.add_argument("--cols", type=int, default=250)
     ap.add_argument("--cpu-sample-outer", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--selector", default="default",
+                    help="learned column selector model for the learned arm ('default': the packaged model, "
+                         "'none': no learned arm)")
+    ap.add_argument("--selector-window", type=float, default=None)
+    ap.add_argument("--selector-steps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -225,6 +234,22 @@ def run_reference(args, rank, world):
     return line
 
 
+def load_selector(args):
+    """The learned arm's model and window: the packaged model (trained on
+    solver traces of other seeds of the same LP family) unless told otherwise."""
+    if args.selector == "none":
+        return None, 0.0
+    from psipm_b200.learned import DEFAULT_MODEL, DEFAULT_WINDOW, SelectorModel
+
+    path = DEFAULT_MODEL if args.selector == "default" else args.selector
+    if not os.path.exists(path):
+        return None, 0.0
+    model = SelectorModel.load(path)
+    model.path = path
+    window = DEFAULT_WINDOW if args.selector_window is None else args.selector_window
+    return model, window
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -238,8 +263,9 @@ def run_ours(args, rank, world, local_rank):
     m, n = lp.A.shape
     dev = NormalEquationsDevice(lp.A, device=local_rank)
 
-    def one_solve():
-        solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev)
+    def one_solve(selector=None, window=0.0):
+        solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev, selector=selector,
+                                                       selector_window=window)
         sol = psipm_solve_resident(lp, solver, tol=args.tol)
         if sol.status != "optimal":
             raise RuntimeError(f"solve ended {sol.status}")
@@ -274,6 +300,25 @@ def run_ours(args, rank, world, local_rank):
     clocks = sampler.stop()
     launches = dev.kernel_launches - launches0
     per_step = max_over_ranks(total / args.steps)
+    # ---- learned column selector (same LP, same timing; the plain rule is `value`) ----
+    learned = None
+    model, window = load_selector(args)
+    if model is not None and args.selector_steps > 0:
+        lt, lpcg, lfb, lref = 0.0, 0, 0, 0
+        for _ in range(args.selector_steps):
+            torch.cuda.synchronize()
+            dev.timer_start()
+            sol_l, solver_l = one_solve(model, window)
+            lt += dev.timer_stop()
+            lpcg += solver_l.pcg_total_iterations
+            lfb += solver_l.selector_fallbacks
+            lref += solver_l.learned_refreshes
+            flush_l2()
+        k = args.selector_steps
+        learned = {"value": max_over_ranks(lt / k), "unit": "s", "steps": k, "model": os.path.basename(model.path),
+                   "window": window, "pcg_iterations_per_step": lpcg / k, "learned_refreshes_per_step": lref / k,
+                   "fallbacks_per_step": lfb / k, "objective": sol_l.obj, "status": sol_l.status,
+                   "speedup_vs_plain": per_step / max_over_ranks(lt / k)}
     # ---- end to end through the public API, host buffers ----------------------
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -328,6 +373,7 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "learned_selector": learned,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "lp_per_s": world / per_step,

@@ -208,8 +208,8 @@ int psipm_solve_dev(psipm_handle* h, const double* r1_dev, const double* r2_dev,
  * proximal centre (xk, yk, zk, wk), the residuals (rd, rp), the
  * complementarity targets (rmz, rmw), a direction D = (dx, dy, dz, dw) and a
  * corrector C = (dxc, dyc, dzc, dwc).  The host keeps only the scalars the
- * loop branches on.  Sums are reproducible to rounding (block partials are
- * combined in no fixed order); minima and maxima are exact.  */
+ * loop branches on.  Sums add block partials in block order (the same bits
+ * on every run); minima and maxima are exact.  */
 
 /* Upload c[n], b[m], u[n] and the masks pos[n], box[n] (0/1 bytes) and
  * allocate the vectors (psipm_active_pool.py:2389-2392). */

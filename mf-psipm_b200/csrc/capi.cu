@@ -45,6 +45,7 @@ void read_thresholds() {
 template <typename T>
 struct FactorStore {
     DevBuf<T> ms, G, update, front, xp, yp, dscp, GT, fvec, dinv;
+    DevBuf<T> fslots, eslots, bslots;  // fixed-order accumulation slots of the apply
 };
 
 template <typename T>
@@ -67,7 +68,7 @@ struct IpmStore {
     DevBuf<double> x, y, z, w, s, xk, yk, zk, wk;
     DevBuf<double> rd, rp, rmz, rmw, r1, zero_m, aty, ax;
     DevBuf<double> dx, dy, dz, dw, dxc, dyc, dzc, dwc;
-    DevBuf<double> red, wref;
+    DevBuf<double> red, wref, part;  // part: per-block partial sums (kIpmPartStride per sum)
     DevBuf<unsigned long long> redu;
     DevBuf<int> flag;
     bool have_ref = false;
@@ -128,6 +129,10 @@ struct psipm_handle {
     DevBuf<BwdTask> bwd_tasks_d;
     std::vector<int> fwd_ptr, bwd_ptr;
     DevBuf<int> fown_d, fdst_d;  // forward-sweep push maps (prec_apply)
+    // fixed-order accumulation of the apply: per front row / update row / column
+    DevBuf<int> frow_nch_d, ecnt_d, brow_nch_d, fcount_d, ecount_d, bcount_d;
+    DevBuf<long long> frow_slot_d, eslot_off_d, uslot_d, brow_slot_d;
+    int64_t nfslots = 0, neslots = 0, nbslots = 0;
     std::vector<int> solve_big_sn;        // supernodes with a transposed panel
     std::vector<int64_t> gt_off_host;
     DevBuf<long long> gt_off_d;
@@ -149,7 +154,8 @@ struct psipm_handle {
     // PCG
     PcgStore<double> p64;
     PcgStore<float> p32;
-    DevBuf<double> x64, r64, rhs64, t64, norm64;  // FP64 refinement (FP32_REFINED)
+    DevBuf<double> x64, r64, rhs64, t64, norm64, norm_part;  // FP64 refinement (FP32_REFINED)
+    DevBuf<double> achunk;                                  // chunk sums of the long rows (a_times)
     DevBuf<double> part;
     DevBuf<int> ctrl, iout;
     DevBuf<unsigned int> gbar;  // grid barrier words of the persistent kernels
@@ -391,6 +397,19 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
         pc.uvec_off = h->s_uvec_off.p;
         pc.fown = h->fown_d.p;
         pc.fdst = h->fdst_d.p;
+        pc.frow_nch = h->frow_nch_d.p;
+        pc.frow_slot = h->frow_slot_d.p;
+        pc.fcount = h->fcount_d.p;
+        pc.fslots = fs.fslots.p;
+        pc.ecnt = h->ecnt_d.p;
+        pc.eslot_off = h->eslot_off_d.p;
+        pc.uslot = h->uslot_d.p;
+        pc.ecount = h->ecount_d.p;
+        pc.eslots = fs.eslots.p;
+        pc.brow_nch = h->brow_nch_d.p;
+        pc.brow_slot = h->brow_slot_d.p;
+        pc.bcount = h->bcount_d.p;
+        pc.bslots = fs.bslots.p;
         pc.nfront = h->sym.sn_rowptr[h->sym.ns];
         pc.nlevels = h->sym.nlevels;
         pc.fwd_ptr = h->fwd_ptr_d.p;
@@ -602,6 +621,61 @@ void analyse(psipm_handle* h) {
         }
         h->fown_d.upload(fown, st);
         h->fdst_d.upload(fdst, st);
+        // slots of the fixed-order accumulation (kernels_pcg.cuh, slot_arrive):
+        //  forward: every GEMV task writes one partial per row of its 4-row group;
+        //  update rows: one slot per (child update row -> parent front row), in
+        //  ascending child and row order; backward: one partial per covering task
+        const int64_t nfront = std::max<int64_t>(1, s.sn_rowptr[s.ns]);
+        std::vector<int> frow_nch(nfront, 0), ecnt(nfront, 0), brow_nch(std::max<int64_t>(1, h->m), 0);
+        std::vector<long long> frow_slot(nfront, 0), eslot_off(nfront + 1, 0), brow_slot(std::max<int64_t>(1, h->m), 0);
+        std::vector<long long> uslot(std::max<int64_t>(1, s.uvec_off[s.ns]), 0);
+        int64_t nf = 0, nb = 0;
+        for (int sn = 0; sn < s.ns; ++sn) {
+            const int first = s.sn_first[sn], c = s.sn_first[sn + 1] - first;
+            const int64_t rb = s.sn_rowptr[sn];
+            const int r = (int)(s.sn_rowptr[sn + 1] - rb);
+            if (r <= kSmallRows && c <= 32) continue;  // fused: rows written directly
+            const int cch = (c + kApplyChunk - 1) / kApplyChunk;
+            for (int i0 = 0; i0 < r; i0 += kApplyRows) {
+                const int i1 = std::min(r, i0 + kApplyRows);
+                const int nch = (i1 - 1 < c) ? (i1 - 1) / kApplyChunk + 1 : cch;
+                for (int ii = i0; ii < i1; ++ii) {
+                    frow_nch[rb + ii] = nch;
+                    frow_slot[rb + ii] = nf;
+                    nf += nch;
+                }
+            }
+            const int rch = (r + kApplyChunk - 1) / kApplyChunk;
+            for (int j0 = 0; j0 < c; j0 += kApplyRows) {
+                const int nch = rch - j0 / kApplyChunk;
+                for (int jj = j0; jj < std::min(c, j0 + kApplyRows); ++jj) {
+                    brow_nch[first + jj] = nch;
+                    brow_slot[first + jj] = nb;
+                    nb += nch;
+                }
+            }
+        }
+        for (int64_t u = 0; u < s.uvec_off[s.ns]; ++u)
+            if (fdst[u] >= 0) ++ecnt[fdst[u]];
+        for (int64_t g = 0; g < nfront; ++g) eslot_off[g + 1] = eslot_off[g] + ecnt[g];
+        {
+            std::vector<long long> fill(eslot_off.begin(), eslot_off.end() - 1);
+            for (int64_t u = 0; u < s.uvec_off[s.ns]; ++u)  // children ascending, rows ascending
+                if (fdst[u] >= 0) uslot[u] = fill[fdst[u]]++;
+        }
+        h->nfslots = std::max<int64_t>(1, nf);
+        h->nbslots = std::max<int64_t>(1, nb);
+        h->neslots = std::max<int64_t>(1, eslot_off[nfront]);
+        h->frow_nch_d.upload(frow_nch, st);
+        h->frow_slot_d.upload(frow_slot, st);
+        h->ecnt_d.upload(ecnt, st);
+        h->eslot_off_d.upload(eslot_off, st);
+        h->uslot_d.upload(uslot, st);
+        h->brow_nch_d.upload(brow_nch, st);
+        h->brow_slot_d.upload(brow_slot, st);
+        h->fcount_d.zero(nfront, st);
+        h->ecount_d.zero(nfront, st);
+        h->bcount_d.zero(std::max<int64_t>(1, h->m), st);
     }
     // per level: fronts factored one per CTA (small) or by the multi-CTA path (big)
     h->small_ptr.assign(s.nlevels + 1, 0);
@@ -638,6 +712,9 @@ void analyse(psipm_handle* h) {
         fs.yp.reserve(h->m);
         fs.dscp.reserve(h->m);
         fs.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
+        fs.fslots.reserve(h->nfslots);
+        fs.eslots.reserve(h->neslots);
+        fs.bslots.reserve(h->nbslots);
         fs.dinv.reserve((int64_t)(s.max_cols / kGB + 1) * kGB * kGB);  // D_J^T blocks of one big front
     };
     if (h->precision != PSIPM_FP64)
@@ -1454,12 +1531,12 @@ __global__ void k_list_rows(int nrows, const int* __restrict__ rows, const int* 
     }
 }
 
-// long rows: one warp per kLongRow-entry chunk, partial sums added with
-// atomics into the zeroed outputs of those rows
+// long rows: one warp per kLongRow-entry chunk writes the chunk's sum; then
+// one warp per long row adds its chunk sums in a fixed order (lane-strided,
+// then a butterfly), so y is the same on every run
 __global__ void k_chunk_rows(int nchunks, const int* __restrict__ cbeg, const int* __restrict__ cend,
-                             const int* __restrict__ crow, const int* __restrict__ idx,
-                             const double* __restrict__ val, const double* __restrict__ v,
-                             double* __restrict__ y) {
+                             const int* __restrict__ idx, const double* __restrict__ val,
+                             const double* __restrict__ v, double* __restrict__ part) {
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -1467,18 +1544,34 @@ __global__ void k_chunk_rows(int nchunks, const int* __restrict__ cbeg, const in
         double acc = 0.0;
         for (int k = cbeg[c] + lane; k < cend[c]; k += 32) acc += val[k] * v[idx[k]];
         acc = warp_sum(acc);
-        if (lane == 0) atomicAdd(&y[crow[c]], acc);
+        if (lane == 0) part[c] = acc;
+    }
+}
+__global__ void k_long_rows(int nlong, const int* __restrict__ rows, const int* __restrict__ chunk_ptr,
+                            const double* __restrict__ part, double* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long l = warp; l < nlong; l += nwarps) {
+        double acc = 0.0;
+        for (int c = chunk_ptr[l] + lane; c < chunk_ptr[l + 1]; c += 32) acc += part[c];
+        acc = warp_sum(acc);
+        if (lane == 0) y[rows[l]] = acc;
     }
 }
 
-__global__ void k_zero_rows(int nrows, const int* __restrict__ rows, double* __restrict__ y) {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < nrows) y[rows[r]] = 0.0;
+// out = sum of part[0 .. n) in a fixed order (one block)
+__global__ void k_fold_sum(long long n, const double* __restrict__ part, double* __restrict__ out) {
+    __shared__ double scratch[32];
+    double acc = 0.0;
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) acc += part[k];
+    acc = block_sum(acc, scratch);
+    if (threadIdx.x == 0) *out = acc;
 }
 
 // y = A v (m rows, FP64) for any row lengths: the short rows by sub-warps
-// sized to their mean length, the long rows in chunks.  Long-row sums are
-// combined with atomics, so y is reproducible to rounding.
+// sized to their mean length, the long rows in chunks whose sums a warp per
+// row adds in a fixed order, so y is the same on every run.
 void a_times(psipm_handle* h, const double* v, double* y) {
     cudaStream_t st = h->stream;
     const int ns = h->n_short;
@@ -1495,10 +1588,12 @@ void a_times(psipm_handle* h, const double* v, double* y) {
             LAUNCH(h, k_list_rows<32><<<grid, 256, 0, st>>>(ns, h->short_rows.p, h->a_ptr.p, h->a_idx.p, h->a_val.p, v, y));
     }
     if (h->n_long) {
-        LAUNCH(h, k_zero_rows<<<blocks_for(h->n_long, 256), 256, 0, st>>>(h->n_long, h->long_rows.p, y));
+        h->achunk.reserve(std::max(1, h->n_chunks));
         const int grid = (int)std::min<int64_t>(blocks_for((int64_t)h->n_chunks * 32, 256), (int64_t)h->num_sms * 16);
-        LAUNCH(h, k_chunk_rows<<<grid, 256, 0, st>>>(h->n_chunks, h->chunk_beg.p, h->chunk_end.p, h->chunk_row.p,
-                                                     h->a_idx.p, h->a_val.p, v, y));
+        LAUNCH(h, k_chunk_rows<<<grid, 256, 0, st>>>(h->n_chunks, h->chunk_beg.p, h->chunk_end.p, h->a_idx.p,
+                                                     h->a_val.p, v, h->achunk.p));
+        LAUNCH(h, k_long_rows<<<blocks_for((int64_t)h->n_long * 32, 256), 256, 0, st>>>(
+                      h->n_long, h->long_rows.p, h->long_chunk_ptr.p, h->achunk.p, y));
     }
 }
 
@@ -1537,7 +1632,7 @@ __global__ void k_at_w(long long n, const int* __restrict__ ptr, const int* __re
     t[j] = w[j] * s;
 }
 
-// r = rhs - (A t + delta x)   (FP64, one warp per row); norm2 += r.r
+// r = rhs - (A t + delta x)   (FP64, one warp per row); per-warp partials of r.r
 __global__ void k_residual(long long m, const int* __restrict__ ptr, const int* __restrict__ idx,
                            const double* __restrict__ val, const double* __restrict__ t, double delta,
                            const double* __restrict__ x, const double* __restrict__ rhs, double* __restrict__ r,
@@ -1556,7 +1651,7 @@ __global__ void k_residual(long long m, const int* __restrict__ ptr, const int* 
         }
     }
     acc = warp_sum(acc);
-    if (lane == 0) atomicAdd(norm2, acc);
+    if (lane == 0) norm2[(blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5] = acc;
 }
 
 __global__ void k_scale_narrow(long long m, const double* __restrict__ r, double s, float* __restrict__ out) {
@@ -1581,12 +1676,13 @@ double fp64_residual(psipm_handle* h, const double* rhs, const double* x) {
     h->t64.reserve(n);
     h->r64.reserve(m);
     h->norm64.reserve(1);
-    PSIPM_CUDA(cudaMemsetAsync(h->norm64.p, 0, sizeof(double), st));
     LAUNCH(h, k_at_w<<<blocks_for(n, 256), 256, 0, st>>>(n, h->at_ptr.p, h->at_idx.p, h->at_val.p, h->w.p, x,
                                                           h->t64.p));
     const int rows = (int)std::min<int64_t>(blocks_for(m * 32, 256), 8 * std::max(1, h->num_sms));
+    h->norm_part.reserve((size_t)rows * 8);
     LAUNCH(h, k_residual<<<rows, 256, 0, st>>>(m, h->a_ptr.p, h->a_idx.p, h->a_val.p, h->t64.p, h->delta, x, rhs,
-                                               h->r64.p, h->norm64.p));
+                                               h->r64.p, h->norm_part.p));
+    LAUNCH(h, k_fold_sum<<<1, 256, 0, st>>>((long long)rows * 8, h->norm_part.p, h->norm64.p));
     double nrm2 = 0.0;
     PSIPM_CUDA(cudaMemcpyAsync(&nrm2, h->norm64.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     PSIPM_CUDA(cudaStreamSynchronize(st));
@@ -1871,7 +1967,8 @@ namespace {
 constexpr int kIpmThreads = 256;
 
 int ipm_grid(const psipm_handle* h, int64_t n) {
-    return (int)std::min<int64_t>(blocks_for(n, kIpmThreads), (int64_t)std::max(1, h->num_sms) * 8);
+    return (int)std::min<int64_t>({blocks_for(n, kIpmThreads), (int64_t)std::max(1, h->num_sms) * 8,
+                                   (int64_t)kIpmPartStride});
 }
 
 void ipm_require(const psipm_handle* h) {
@@ -1895,7 +1992,14 @@ void spmv_csr(psipm_handle* h, int64_t rows, int64_t nnz, const int* ptr, const 
 }
 
 void ipm_reset(psipm_handle* h, int nred, int nu, unsigned long long uval) {
+    if (nred)
+        PSIPM_CUDA(cudaMemsetAsync(h->ipm.part.p, 0, (size_t)nred * kIpmPartStride * sizeof(double), h->stream));
     LAUNCH(h, k_ipm_reset<<<1, 32, 0, h->stream>>>(h->ipm.red.p, nred, h->ipm.redu.p, nu, uval, h->ipm.flag.p));
+}
+
+// the sums' block partials -> red[0 .. nred), in block order
+void ipm_fold(psipm_handle* h, int nred) {
+    LAUNCH(h, k_ipm_fold<<<1, 32, 0, h->stream>>>(nred, h->ipm.part.p, h->ipm.red.p));
 }
 
 unsigned long long bits_of(double v) {
@@ -1954,6 +2058,7 @@ int psipm_ipm_load(psipm_handle* h, const double* c, const double* b, const doub
             v->zero(n, st);
         for (DevBuf<double>* v : {&I.y, &I.yk, &I.rp, &I.zero_m, &I.ax, &I.dy, &I.dyc}) v->zero(m, st);
         I.red.zero(8, st);
+        I.part.zero((size_t)8 * kIpmPartStride, st);
         I.redu.zero(4, st);
         I.flag.zero(1, st);
         I.loaded = true;
@@ -2017,12 +2122,14 @@ int psipm_ipm_residuals(psipm_handle* h, double rho, double delta, double* out) 
         ipm_products(h);
         ipm_reset(h, 8, 0, 0ull);
         LAUNCH(h, k_ipm_residual_n<<<ipm_grid(h, n), kIpmThreads, 0, st>>>(
-                      n, I.c.p, I.aty.p, I.x.p, I.z.p, I.w.p, I.xk.p, I.u.p, I.pos.p, rho, I.rd.p, I.red.p + 1));
+                      n, I.c.p, I.aty.p, I.x.p, I.z.p, I.w.p, I.xk.p, I.u.p, I.pos.p, rho, I.rd.p,
+                      I.part.p + 1 * kIpmPartStride));
         LAUNCH(h, k_ipm_residual_m<<<ipm_grid(h, m), kIpmThreads, 0, st>>>(m, I.ax.p, I.b.p, I.y.p, I.yk.p, delta,
-                                                                            I.rp.p, I.red.p + 1));
+                                                                            I.rp.p, I.part.p + 1 * kIpmPartStride));
         LAUNCH(h, k_ipm_comp<<<ipm_grid(h, n), kIpmThreads, 0, st>>>(
                       n, I.x.p, I.s.p, I.z.p, I.w.p, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0,
-                      0.0, I.pos.p, I.box.p, I.red.p));
+                      0.0, I.pos.p, I.box.p, I.part.p));
+        ipm_fold(h, 6);
         read_back(h, out, I.red.p, 6);
     });
 }
@@ -2243,7 +2350,8 @@ int psipm_ipm_complementarity(psipm_handle* h, int32_t with_corrector, double ga
         LAUNCH(h, k_ipm_comp<<<ipm_grid(h, h->n), kIpmThreads, 0, h->stream>>>(
                       h->n, I.x.p, I.s.p, I.z.p, I.w.p, I.dx.p, I.dz.p, I.dw.p, c ? I.dxc.p : nullptr,
                       c ? I.dzc.p : nullptr, c ? I.dwc.p : nullptr, gamma, alpha_x, alpha_z, I.pos.p, I.box.p,
-                      I.red.p));
+                      I.part.p));
+        ipm_fold(h, 1);
         read_back(h, out, I.red.p, 1);
     });
 }
@@ -2278,10 +2386,11 @@ int psipm_ipm_metrics(psipm_handle* h, double* out) {
         ipm_products(h);
         ipm_reset(h, 4, 2, 0ull);
         LAUNCH(h, k_ipm_outer_n<<<ipm_grid(h, h->n), kIpmThreads, 0, st>>>(h->n, I.c.p, I.aty.p, I.x.p, I.z.p, I.w.p,
-                                                                            I.s.p, I.u.p, I.pos.p, I.box.p, I.red.p,
+                                                                            I.s.p, I.u.p, I.pos.p, I.box.p, I.part.p,
                                                                             I.redu.p));
-        LAUNCH(h, k_ipm_outer_m<<<ipm_grid(h, h->m), kIpmThreads, 0, st>>>(h->m, I.ax.p, I.b.p, I.y.p, I.red.p,
+        LAUNCH(h, k_ipm_outer_m<<<ipm_grid(h, h->m), kIpmThreads, 0, st>>>(h->m, I.ax.p, I.b.p, I.y.p, I.part.p,
                                                                             I.redu.p));
+        ipm_fold(h, 4);
         double sums[4];
         unsigned long long mx[2];
         PSIPM_CUDA(cudaMemcpyAsync(sums, I.red.p, sizeof(sums), cudaMemcpyDeviceToHost, st));
@@ -2360,7 +2469,7 @@ __global__ void k_dot(long long len, const double* __restrict__ x, const double*
          j += (long long)gridDim.x * blockDim.x)
         acc += x[j] * y[j];
     acc = block_sum(acc, scratch);
-    if (threadIdx.x == 0) atomicAdd(out, acc);
+    if (threadIdx.x == 0) out[blockIdx.x] = acc;  // one partial per block
 }
 
 struct MinresState {
@@ -2387,8 +2496,10 @@ struct MinresState {
                                                                                            out));
     }
     double dot(const double* x, const double* y) {
-        PSIPM_CUDA(cudaMemsetAsync(W.dot.p, 0, sizeof(double), h->stream));
-        LAUNCH(h, k_dot<<<ipm_grid(h, len), kIpmThreads, 0, h->stream>>>(len, x, y, W.dot.p));
+        const int g = ipm_grid(h, len);
+        W.dot.reserve((size_t)g + 1);
+        LAUNCH(h, k_dot<<<g, kIpmThreads, 0, h->stream>>>(len, x, y, W.dot.p + 1));
+        LAUNCH(h, k_fold_sum<<<1, 256, 0, h->stream>>>(g, W.dot.p + 1, W.dot.p));
         double v = 0.0;
         read_back(h, &v, W.dot.p, 1);
         return v;

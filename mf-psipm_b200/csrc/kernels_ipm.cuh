@@ -8,10 +8,11 @@
 // plus the Gondzio corrector targets and the iterate update with the box
 // floors (psipm_active_pool.py:1845-1872).  Masks `pos` / `box` are uint8.
 //
-// Reductions: sums go through a block sum and one atomicAdd per block (the
-// order of the block partials is not fixed, so totals are reproducible to
-// rounding); minima of nonnegative doubles use atomicMin on their bit
-// patterns, which order like the values.
+// Reductions: sums go through a block sum that each block writes to its own
+// slot (slot k of a sum at part[k * kIpmPartStride + block]); k_ipm_fold adds
+// the slots in block order, so every total is the same on every run.  Minima
+// of nonnegative doubles use atomicMin on their bit patterns, which order like
+// the values (exact in any order).
 #pragma once
 
 #include "common.cuh"
@@ -20,9 +21,20 @@ namespace psipm {
 
 constexpr double kPosFloor = 8.0 * 2.220446049250313e-16;  // psipm_active_pool.py:61
 
+constexpr int kIpmPartStride = 4096;  // >= the largest grid of the IPM kernels
+
 __device__ __forceinline__ void block_add(double v, double* out, double* scratch) {
     v = block_sum(v, scratch);
-    if (threadIdx.x == 0) atomicAdd(out, v);
+    if (threadIdx.x == 0) out[blockIdx.x] = v;
+}
+
+// red[k] = sum over b < kIpmPartStride of part[k * kIpmPartStride + b], in order
+__global__ void k_ipm_fold(int nred, const double* __restrict__ part, double* __restrict__ red) {
+    const int k = threadIdx.x;
+    if (k >= nred) return;
+    double s = 0.0;
+    for (int b = 0; b < kIpmPartStride; ++b) s += part[(long long)k * kIpmPartStride + b];
+    red[k] = s;
 }
 
 // minimum of nonnegative values through their (monotone) bit patterns
@@ -271,9 +283,9 @@ __global__ void k_ipm_residual_n(long long n, const double* __restrict__ c, cons
         a2 += r * r;
         a3 += dxk * dxk;
     }
-    block_add(a0, out + 0, scratch);
-    block_add(a2, out + 2, scratch);
-    block_add(a3, out + 3, scratch);
+    block_add(a0, out + 0 * kIpmPartStride, scratch);
+    block_add(a2, out + 2 * kIpmPartStride, scratch);
+    block_add(a3, out + 3 * kIpmPartStride, scratch);
 }
 
 __global__ void k_ipm_residual_m(long long m, const double* __restrict__ ax, const double* __restrict__ b,
@@ -289,8 +301,8 @@ __global__ void k_ipm_residual_m(long long m, const double* __restrict__ ax, con
         a1 += r * r;
         a4 += dyk * dyk;
     }
-    block_add(a1, out + 1, scratch);
-    block_add(a4, out + 4, scratch);
+    block_add(a1, out + 1 * kIpmPartStride, scratch);
+    block_add(a4, out + 4 * kIpmPartStride, scratch);
 }
 
 // outer KKT measures (psipm_active_pool.py:2561-2599), given aty and ax:
@@ -315,9 +327,9 @@ __global__ void k_ipm_outer_n(long long n, const double* __restrict__ c, const d
             comp += s[j] * w[j];
         }
     }
-    block_add(cx, out + 0, scratch);
-    block_add(wu, out + 2, scratch);
-    block_add(comp, out + 3, scratch);
+    block_add(cx, out + 0 * kIpmPartStride, scratch);
+    block_add(wu, out + 2 * kIpmPartStride, scratch);
+    block_add(comp, out + 3 * kIpmPartStride, scratch);
     unsigned long long bm = (unsigned long long)__double_as_longlong(rdmax);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -337,7 +349,7 @@ __global__ void k_ipm_outer_m(long long m, const double* __restrict__ ax, const 
         by += b[i] * y[i];
         rpmax = nan_max(rpmax, fabs(b[i] - ax[i]));
     }
-    block_add(by, out + 1, scratch);
+    block_add(by, out + 1 * kIpmPartStride, scratch);
     unsigned long long bm = (unsigned long long)__double_as_longlong(rpmax);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

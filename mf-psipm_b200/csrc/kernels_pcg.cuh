@@ -147,6 +147,22 @@ struct PrecLayout {
     int trace_cap = 0;
     T* xp = nullptr;
     T* yp = nullptr;
+    // fixed-order accumulation (no floating-point atomics): every partial sum
+    // goes to its own slot and the contributor that completes a destination
+    // (an atomic arrival count) adds the slots in slot order
+    const int* frow_nch = nullptr;       // per front row: forward tasks that cover it (0: fused supernode)
+    const long long* frow_slot = nullptr;
+    int* fcount = nullptr;               // per front row: arrivals
+    T* fslots = nullptr;
+    const int* ecnt = nullptr;           // per front row: child update rows that add into it
+    const long long* eslot_off = nullptr;
+    const long long* uslot = nullptr;    // per update row: its slot in the parent's list
+    int* ecount = nullptr;
+    T* eslots = nullptr;
+    const int* brow_nch = nullptr;       // per permuted column: backward tasks that cover it (0: fused)
+    const long long* brow_slot = nullptr;
+    int* bcount = nullptr;
+    T* bslots = nullptr;
     // extracted dense columns: the Woodbury correction of the apply (lr_q = 0: none)
     int lr_q = 0;
     const int* lr_ptr = nullptr;      // q + 1 offsets into lr_row / lr_val
@@ -333,10 +349,14 @@ __device__ void phase_b2(const PcgArgs<T, P>& a, int mode, int src, T beta, doub
 //                                 x_s = G_top f_top,  u_s = f_bot - G_bot f_top
 //   backward (levels top-down):   v = [x_s ; -y(rows below)]
 //                                 y_s = G^T v
-// The forward sweep pushes: every supernode adds its u_s straight into its
-// parent's f (fvec at fdst) with atomics, so a level needs no gather phase,
-// and one flat pass before the first level writes every f = [b_s ; 0] and
-// clears x, y.  The backward sweep gathers v into registers inside each task.
+// The forward sweep pushes: every supernode's update rows u_s go to their
+// parent's f (fvec at fdst), so a level needs no gather phase, and one flat
+// pass before the first level writes every f = [b_s ; 0], clears x, y and
+// the arrival counts.  No floating-point atomics: each partial sum (a chunk of
+// a row, a child's update row) is stored in its own slot, and whichever
+// contributor completes a destination adds that destination's slots in slot
+// order, so an application gives the same bits on every run.  The backward
+// sweep gathers v into registers inside each task.
 // Big supernodes are cut into 2-D tasks of kApplyRows output rows x
 // kApplyChunk contraction entries; each lane holds kLaneCols entries of the
 // vector chunk and loads its kLaneCols columns of four rows at once.
@@ -371,6 +391,37 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// Slot protocol: store this contribution in its slot; when the destination
+// expects more than one, publish it (fence, arrival count) and report whether
+// this was the last one, which then sees every slot (fence) and sums them in
+// slot order.
+template <typename P>
+__device__ __forceinline__ bool slot_arrive(P* slots, long long slot, P v, int expected, int* count) {
+    slots[slot] = v;
+    if (expected <= 1) return true;
+    __threadfence();
+    const bool last = atomicAdd(count, 1) == expected - 1;
+    if (last) __threadfence();
+    return last;
+}
+template <typename P>
+__device__ __forceinline__ P slot_sum(const P* slots, long long base, int count, P init) {
+    P s = init;
+    for (int k = 0; k < count; ++k) s += __ldcg(slots + base + k);
+    return s;
+}
+
+// An update row u of a child adds into its parent's front row fdst[u]; the
+// last of the parent row's contributors writes f = base + sum of the slots.
+template <typename P>
+__device__ __forceinline__ void deliver_update(const PrecLayout<P>& pc, long long u, P val) {
+    const int e = pc.fdst[u];
+    if (e < 0) return;
+    const int ne = pc.ecnt[e];
+    if (slot_arrive(pc.eslots, pc.uslot[u], val, ne, pc.ecount + e))
+        pc.fvec[e] = slot_sum(pc.eslots, pc.eslot_off[e], ne, __ldcg(pc.fvec + e));
+}
+
 // forward task: rows [i0, i1) (at most four) of G against f[j0, j0 + kApplyChunk).
 // Every lane loads a clamped in-row index and masks the product, so the
 // sixteen loads carry no branches and issue together.
@@ -381,15 +432,7 @@ __device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t) {
     const P* __restrict__ G = pc.G + t.g;
     const P* f = pc.fvec + t.f;
     const int j1 = min(c, j0 + kApplyChunk);
-    // epilogue operands of lane k < 4 (row i0 + k), loaded up front
-    const int ii = i0 + lane;
-    const bool bottom = lane < 4 && ii < i1 && ii >= c;
-    int e = -1;
-    P fb = 0;
-    if (bottom) {
-        e = pc.fdst[t.u + ii - c];
-        fb = j0 == 0 ? f[ii] : (P)0;
-    }
+    const int ii = i0 + lane;  // the row lane k < 4 finishes
     P fr[kLaneCols];
 #pragma unroll
     for (int q = 0; q < kLaneCols; ++q) {
@@ -415,10 +458,17 @@ __device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t) {
     }
     const P v = warp_sum4(d);
     if (lane < 4 && ii < i1) {
-        if (ii < c)
-            atomicAdd(&pc.xp[t.first + ii], v);
-        else if (e >= 0)
-            atomicAdd(&pc.fvec[e], fb - v);  // u pushed into the parent's front vector
+        // this chunk's part of row ii; the row's last chunk finishes it:
+        // x = G_top f_top (pivot rows), u = f_bot - G_bot f_top (update rows)
+        const long long g = t.f + ii;
+        const int nch = pc.frow_nch[g];
+        if (slot_arrive(pc.fslots, pc.frow_slot[g] + j0 / kApplyChunk, v, nch, pc.fcount + g)) {
+            const P sum = slot_sum(pc.fslots, pc.frow_slot[g], nch, (P)0);
+            if (ii < c)
+                pc.xp[t.first + ii] = sum;
+            else
+                deliver_update(pc, t.u + ii - c, __ldcg(pc.fvec + g) - sum);
+        }
     }
 }
 
@@ -451,7 +501,13 @@ __device__ void prec_backward_gemv(const PrecLayout<P>& pc, const BwdTask& t) {
         d[k] = acc;
     }
     const P v = warp_sum4(d);
-    if (lane < 4 && j0 + lane < j1) atomicAdd(&pc.yp[t.first + j0 + lane], v);
+    if (lane < 4 && j0 + lane < j1) {
+        const int col = t.first + j0 + lane;
+        const int nch = pc.brow_nch[col];
+        if (slot_arrive(pc.bslots, pc.brow_slot[col] + (i0 / kApplyChunk - j0 / kApplyChunk), v, nch,
+                        pc.bcount + col))
+            pc.yp[col] = slot_sum(pc.bslots, pc.brow_slot[col], nch, (P)0);
+    }
 }
 
 // Small supernodes (r <= kSmallRows, c <= 32): one warp does the whole
@@ -476,12 +532,10 @@ __device__ void prec_forward_small(const PrecLayout<P>& pc, int s, P* fs) {
         P d = 0;
 #pragma unroll 8
         for (int j = 0; j < jlim; ++j) d += g[j] * fs[j];
-        if (row < c) {
+        if (row < c)
             pc.xp[first + row] = d;
-        } else {
-            const int dst = pc.fdst[uo + row - c];
-            if (dst >= 0) atomicAdd(&pc.fvec[dst], fs[row] - d);
-        }
+        else
+            deliver_update(pc, uo + row - c, fs[row] - d);
     }
     __syncwarp();
 }
@@ -619,9 +673,14 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
         const int k = pc.fown[g];
         pc.fvec[g] = k >= 0 ? pc.dscp[k] * (P)in[pc.perm[k]] : (P)0;
     }
+    for (long long g = gtid; g < pc.nfront; g += gstride) {
+        pc.fcount[g] = 0;
+        pc.ecount[g] = 0;
+    }
     for (int k = gtid; k < pc.m; k += gstride) {
         pc.xp[k] = 0;
         pc.yp[k] = 0;
+        pc.bcount[k] = 0;
     }
     grid.sync();
     mark();

@@ -16,9 +16,9 @@ projection) runs on the device as well: the policy factors theta = 1, the two
 projections go straight into the device iterate (``solve_start``) and
 ``psipm_ipm_start`` forms the shifted start there.
 
-Sums that the loop branches on are folded from block partials; the
-preconditioner application adds with atomics, so the trajectory is
-reproducible to rounding, not bit for bit.
+Every sum the loop branches on adds block partials in a fixed order and the
+preconditioner application accumulates through fixed-order slots, so a solve
+takes the same trajectory, bit for bit, on every run.
 """
 
 from __future__ import annotations

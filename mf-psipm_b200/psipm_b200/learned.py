@@ -46,6 +46,9 @@ from . import _lib
 
 N_IN, N_HID, N_OUT = _lib.MLP_INPUTS, 64, 2
 N_WEIGHTS, N_BIASES, N_PARAMS = _lib.MLP_WEIGHTS, _lib.MLP_BIASES, _lib.MLP_PARAMS
+# packaged model: trained on device traces of 200 x 250 grid networks (seeds 1100-1111)
+DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "selector_grid.npz")
+DEFAULT_WINDOW = 0.0
 
 
 def _bf16_bits(x: np.ndarray) -> np.ndarray:
@@ -356,3 +359,4 @@ def main(argv=None) -> None:
 
 if __name__ == "__main__":
     main()
+

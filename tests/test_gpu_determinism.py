@@ -1,0 +1,85 @@
+"""Run-to-run determinism of the device path, and the refresh/refactor
+trajectory (row H5, psipm_spectral_preconditioner.py:420-467) against the
+reference's.
+
+The preconditioner application accumulates through fixed-order slots and
+every reduction adds block partials in block order, so:
+* two applications of the same factor give the same bits;
+* two device-resident solves of the same LP take the same trajectory: the
+  same PCG iteration counts, core sizes, factorisations and objective bits
+  (a grid network and a set-cover LP, whose long rows go through the chunked
+  row sums).
+Against the reference's own run (fixtures of tests/golden/make_golden.py),
+the device solver driven by the reference's outer loop takes the same
+refresh/refactor decisions: the same core sizes and number of
+factorisations, and PCG iteration counts within one of the reference's.
+"""
+
+import numpy as np
+import pytest
+
+from _helpers import NAMES, OPTIONS, lp_from
+
+pytestmark = pytest.mark.gpu
+
+
+def test_apply_gives_the_same_bits_twice():
+    from psipm_b200 import synthetic
+    from psipm_b200.device import NormalEquationsDevice
+
+    lp = synthetic.grid_network(60, 80, seed=5)
+    dev = NormalEquationsDevice(lp.A)
+    try:
+        rng = np.random.default_rng(1)
+        dev.set_theta(np.exp(rng.uniform(-6, 6, lp.A.shape[1])), 1e-8)
+        dev.set_core(np.sort(rng.choice(dev.candidates, 2 * lp.A.shape[0], replace=False)))
+        dev.factor(1e-8, 0)
+        r = rng.standard_normal(lp.A.shape[0])
+        z1, z2 = dev.apply(r), dev.apply(r)
+        assert np.array_equal(z1, z2)
+        v = rng.standard_normal(lp.A.shape[0])
+        assert np.array_equal(dev.matvec(v), dev.matvec(v))
+    finally:
+        dev.close()
+
+
+@pytest.mark.parametrize("family", ["grid", "cover"])
+def test_two_solves_take_the_same_trajectory(family):
+    from psipm_b200 import synthetic
+    from psipm_b200.ipm_device import solve_standard
+
+    lp = (synthetic.grid_network(60, 80, seed=6) if family == "grid"
+          else synthetic.set_cover(400, 20_000, seed=2001))
+    runs = []
+    for _ in range(2):
+        sol, solver = solve_standard(lp, tol=1e-8)
+        runs.append((sol, list(solver.cg_iterations), list(solver.core_sizes), solver.n_fact))
+        solver.close()
+    (s1, it1, cs1, nf1), (s2, it2, cs2, nf2) = runs
+    print(f"{family}: {s1.status}, outer {s1.outer_iter}, PCG {sum(it1)}, factorisations {nf1}")
+    assert s1.status == "optimal"
+    assert it1 == it2 and cs1 == cs2 and nf1 == nf2
+    assert s1.obj == s2.obj and np.array_equal(s1.x, s2.x)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_refresh_and_refactor_decisions_follow_the_reference(name, golden):
+    from oracle import ipm as OI
+    from psipm_b200.kkt import GpuSpectralStableColumnPreconditioner
+
+    g = golden(name)
+    lp = lp_from(g)
+    solver = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, **OPTIONS)
+    try:
+        sol = OI.psipm_solve(lp, solver, tol=1e-8)
+        ref_it, ref_cs = list(g["cg_iterations"]), list(g["core_sizes"])
+        it, cs = list(solver.cg_iterations), list(solver.core_sizes)
+        k = next((i for i, (a, b) in enumerate(zip(it, ref_it)) if abs(a - b) > 1), min(len(it), len(ref_it)))
+        print(f"{name}: solves {len(it)} (reference {len(ref_it)}), factorisations {solver.n_fact} "
+              f"(reference {int(g['n_fact'])}), PCG counts within one of the reference's for the first {k} solves")
+        assert sol.status == "optimal"
+        assert cs == ref_cs
+        assert solver.n_fact == int(g["n_fact"])
+        assert len(it) == len(ref_it) and k == len(it)
+    finally:
+        solver.close()
