@@ -72,6 +72,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--workload", choices=("grid", "batch"), default="grid",
+                    help="grid: the 200x250 network LP (the default line); batch: uneven random LPs "
+                         "served several at a time, against the same LPs one after another")
+    ap.add_argument("--count", type=int, default=256, help="LPs of the batch workload")
+    ap.add_argument("--workers", type=int, default=8, help="LPs in flight in the batch workload")
     ap.add_argument("--rows", type=int, default=200)
     ap.add_argument("--cols", type=int, default=250)
     ap.add_argument("--cpu-sample-outer", type=int, default=2)
@@ -381,6 +386,38 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def run_batch(args, rank, world, local_rank):
+    """Uneven random LPs (m ~ U{500..5000}, n = 3m, seeded) on this rank's GPU:
+    the whole batch with --workers LPs in flight, then the same LPs one after
+    another; value = batched LPs per second (nnz-balanced shares per rank)."""
+    import torch
+
+    from psipm_b200 import synthetic
+    from psipm_b200.batch import solve_batch, solve_sequential
+    from psipm_b200.replicas import max_over_ranks, partition_by_nnz
+
+    torch.cuda.set_device(local_rank)
+    lps = synthetic.random_lp_batch(count=args.count, seed=4000)
+    mine = [lps[k] for k in partition_by_nnz([lp.A.nnz for lp in lps], world)[rank]]
+    solve_batch(mine[: min(len(mine), args.workers)], workers=args.workers, device=local_rank)  # warm-up
+    bat = solve_batch(mine, workers=args.workers, device=local_rank)
+    seconds = max_over_ranks(bat.seconds)
+    seq = solve_sequential(mine, device=local_rank) if world == 1 else None
+    if rank != 0:
+        return None
+    return {
+        "metric": "LPs solved to 1e-8 per second (batched serving)", "value": len(lps) / seconds,
+        "unit": "LP/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * seconds,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(lps)} uneven random LPs, m ~ U{{500..5000}}, n = 3m, 5 nonzeros per column, "
+                               f"seeds 4001..{4000 + len(lps)}", "workers": args.workers, "tol": 1e-8},
+        "p50_s": bat.percentile(50), "p99_s": bat.percentile(99),
+        "optimal": sum(s == "optimal" for s in bat.status), "errors": bat.errors[:5],
+        "sequential": None if seq is None else {"value": seq.lps_per_second, "p50_s": seq.percentile(50),
+                                                "p99_s": seq.percentile(99), "seconds": seq.seconds},
+    }
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -398,6 +435,8 @@ def main():
     try:
         if args.impl == "reference":
             line = run_reference(args, rank, world)
+        elif args.workload == "batch":
+            line = run_batch(args, rank, world, local_rank)
         else:
             line = run_ours(args, rank, world, local_rank)
         if rank == 0 and line is not None:

@@ -133,6 +133,20 @@ int psipm_scores(psipm_handle* h, double fill_weight, double* scores, double* di
 int psipm_refresh_core(psipm_handle* h, int64_t target, double retention, int32_t stable,
                        const int64_t* mandatory_local, int64_t nmandatory,
                        int64_t* core_out, int64_t* ncore, double* retained);
+/* Deterministic preconditioner applications (on != 0): the partial sums of
+ * the triangular sweeps go to their own slots and are added in a fixed
+ * order, so a PCG and a whole IPM solve take the same trajectory, bit for
+ * bit, on every run.  Off (the default): FP64 atomics, faster; the order of
+ * the additions, and so the last bits and possibly an iteration count, can
+ * change between runs.  Every other reduction of the library has a fixed
+ * order in both modes. */
+int psipm_set_deterministic(psipm_handle* h, int32_t on);
+/* Grid of this handle's persistent kernels (PCG, apply, operator): `blocks`
+ * thread blocks (at most the co-resident maximum chosen at creation; 0 goes
+ * back to it).  Several handles that solve small LPs concurrently on their
+ * own streams each take a share of the GPU this way (psipm_b200.batch).  Not
+ * with extracted dense columns (PSIPM_ERR_STATE). */
+int psipm_set_grid(psipm_handle* h, int32_t blocks);
 /* Straddling ties of the top-k selections (psipm_refresh_core, psipm_top_k).
  * The reference selects with np.argpartition (psipm_stable_preconditioner.py:
  * 97-110), whose pick among equal scores that straddle the cut depends on

@@ -86,6 +86,8 @@ struct psipm_handle {
     int64_t launches = 0;
     int num_sms = 0;
     int coop_blocks = 0;
+    int coop_max = 0;  // the largest co-resident grid of the persistent kernels
+    bool deterministic = false;  // fixed-order accumulation in the preconditioner apply
 
     // A in CSC on the host (needed by the symbolic analysis)
     std::vector<int64_t> colptr;
@@ -397,6 +399,7 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
         pc.uvec_off = h->s_uvec_off.p;
         pc.fown = h->fown_d.p;
         pc.fdst = h->fdst_d.p;
+        pc.deterministic = h->deterministic ? 1 : 0;
         pc.frow_nch = h->frow_nch_d.p;
         pc.frow_slot = h->frow_slot_d.p;
         pc.fcount = h->fcount_d.p;
@@ -1189,6 +1192,7 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
         int want = 4;
         if (const char* v = std::getenv("PSIPM_BLOCKS_PER_SM")) want = std::max(1, std::atoi(v));
         h->coop_blocks = std::min(per_sm, want) * h->num_sms;
+        h->coop_max = h->coop_blocks;
         build_matrix(h.get());
     });
     if (rc != PSIPM_OK) {
@@ -1388,6 +1392,19 @@ int psipm_refresh_core(psipm_handle* h, int64_t target, double retention, int32_
         *ncore = (int64_t)newcore.size();
         set_core_internal(h, std::move(newcore));
     });
+}
+
+int psipm_set_deterministic(psipm_handle* h, int32_t on) {
+    if (!h) return PSIPM_ERR_ARGUMENT;
+    h->deterministic = on != 0;
+    return PSIPM_OK;
+}
+
+int psipm_set_grid(psipm_handle* h, int32_t blocks) {
+    if (!h || blocks < 0) return PSIPM_ERR_ARGUMENT;
+    if (h->lr_ready || !h->lr_cols.empty()) return PSIPM_ERR_STATE;  // lr_part is sized for the grid
+    h->coop_blocks = blocks == 0 ? h->coop_max : std::min(blocks, h->coop_max);
+    return PSIPM_OK;
 }
 
 int psipm_tie_info(const psipm_handle* h, int64_t* out) {

@@ -147,9 +147,12 @@ struct PrecLayout {
     int trace_cap = 0;
     T* xp = nullptr;
     T* yp = nullptr;
-    // fixed-order accumulation (no floating-point atomics): every partial sum
-    // goes to its own slot and the contributor that completes a destination
-    // (an atomic arrival count) adds the slots in slot order
+    // fixed-order accumulation (deterministic != 0; no floating-point atomics):
+    // every partial sum goes to its own slot and the contributor that completes
+    // a destination (an atomic arrival count) adds the slots in slot order.
+    // Otherwise partial sums are added with FP64 atomics (faster; the order,
+    // and so the last bits, can change from run to run).
+    int deterministic = 0;
     const int* frow_nch = nullptr;       // per front row: forward tasks that cover it (0: fused supernode)
     const long long* frow_slot = nullptr;
     int* fcount = nullptr;               // per front row: arrivals
@@ -351,12 +354,13 @@ __device__ void phase_b2(const PcgArgs<T, P>& a, int mode, int src, T beta, doub
 //                                 y_s = G^T v
 // The forward sweep pushes: every supernode's update rows u_s go to their
 // parent's f (fvec at fdst), so a level needs no gather phase, and one flat
-// pass before the first level writes every f = [b_s ; 0], clears x, y and
-// the arrival counts.  No floating-point atomics: each partial sum (a chunk of
-// a row, a child's update row) is stored in its own slot, and whichever
-// contributor completes a destination adds that destination's slots in slot
-// order, so an application gives the same bits on every run.  The backward
-// sweep gathers v into registers inside each task.
+// pass before the first level writes every f = [b_s ; 0] and clears x, y (and
+// the arrival counts).  Partial sums (a chunk of a row, a child's update row)
+// are added with FP64 atomics, or, on a handle set to be deterministic, each
+// is stored in its own slot and whichever contributor completes a destination
+// adds that destination's slots in slot order, so an application gives the
+// same bits on every run.  The backward sweep gathers v into registers inside
+// each task.
 // Big supernodes are cut into 2-D tasks of kApplyRows output rows x
 // kApplyChunk contraction entries; each lane holds kLaneCols entries of the
 // vector chunk and loads its kLaneCols columns of four rows at once.
@@ -417,6 +421,10 @@ template <typename P>
 __device__ __forceinline__ void deliver_update(const PrecLayout<P>& pc, long long u, P val) {
     const int e = pc.fdst[u];
     if (e < 0) return;
+    if (!pc.deterministic) {
+        atomicAdd(&pc.fvec[e], val);
+        return;
+    }
     const int ne = pc.ecnt[e];
     if (slot_arrive(pc.eslots, pc.uslot[u], val, ne, pc.ecount + e))
         pc.fvec[e] = slot_sum(pc.eslots, pc.eslot_off[e], ne, __ldcg(pc.fvec + e));
@@ -457,7 +465,12 @@ __device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t) {
         d[k] = acc;
     }
     const P v = warp_sum4(d);
-    if (lane < 4 && ii < i1) {
+    if (lane < 4 && ii < i1 && !pc.deterministic) {
+        if (ii < c)
+            atomicAdd(&pc.xp[t.first + ii], v);
+        else  // u pushed into the parent's front vector; f_bot once, with the first chunk
+            deliver_update(pc, t.u + ii - c, (j0 == 0 ? f[ii] : (P)0) - v);
+    } else if (lane < 4 && ii < i1) {
         // this chunk's part of row ii; the row's last chunk finishes it:
         // x = G_top f_top (pivot rows), u = f_bot - G_bot f_top (update rows)
         const long long g = t.f + ii;
@@ -501,7 +514,9 @@ __device__ void prec_backward_gemv(const PrecLayout<P>& pc, const BwdTask& t) {
         d[k] = acc;
     }
     const P v = warp_sum4(d);
-    if (lane < 4 && j0 + lane < j1) {
+    if (lane < 4 && j0 + lane < j1 && !pc.deterministic) {
+        atomicAdd(&pc.yp[t.first + j0 + lane], v);
+    } else if (lane < 4 && j0 + lane < j1) {
         const int col = t.first + j0 + lane;
         const int nch = pc.brow_nch[col];
         if (slot_arrive(pc.bslots, pc.brow_slot[col] + (i0 / kApplyChunk - j0 / kApplyChunk), v, nch,
@@ -673,14 +688,15 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
         const int k = pc.fown[g];
         pc.fvec[g] = k >= 0 ? pc.dscp[k] * (P)in[pc.perm[k]] : (P)0;
     }
-    for (long long g = gtid; g < pc.nfront; g += gstride) {
-        pc.fcount[g] = 0;
-        pc.ecount[g] = 0;
-    }
+    if (pc.deterministic)
+        for (long long g = gtid; g < pc.nfront; g += gstride) {
+            pc.fcount[g] = 0;
+            pc.ecount[g] = 0;
+        }
     for (int k = gtid; k < pc.m; k += gstride) {
         pc.xp[k] = 0;
         pc.yp[k] = 0;
-        pc.bcount[k] = 0;
+        if (pc.deterministic) pc.bcount[k] = 0;
     }
     grid.sync();
     mark();

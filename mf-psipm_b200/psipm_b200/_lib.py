@@ -106,6 +106,8 @@ SIGNATURES = {
     "psipm_refresh_core": (_I32, [_P, _I64, _D, _I32, _P, _I64, _P, _P, _P]),
     "psipm_set_core": (_I32, [_P, _P, _I64]),
     "psipm_tie_info": (_I32, [_P, _P]),
+    "psipm_set_grid": (_I32, [_P, _I32]),
+    "psipm_set_deterministic": (_I32, [_P, _I32]),
     "psipm_top_k": (_I32, [_P, _P, _I64, _P, _I64, _P, _P]),
     "psipm_factor": (_I32, [_P, _D, _I32, _P, _P]),
     "psipm_apply": (_I32, [_P, _P, _P]),

@@ -194,6 +194,14 @@ class NormalEquationsDevice:
         self._check(self.lib.psipm_mlp_scores(self.h, ptr(w), ptr(b), float(mu), int(keep), ctypes.byref(vote)))
         return float(vote.value)
 
+    def set_deterministic(self, on: bool) -> None:
+        """Fixed-order accumulation in the preconditioner apply (psipm_set_deterministic)."""
+        self._check(self.lib.psipm_set_deterministic(self.h, int(bool(on))))
+
+    def set_grid(self, blocks: int) -> None:
+        """Blocks of this handle's persistent kernels (0: the full co-resident grid)."""
+        self._check(self.lib.psipm_set_grid(self.h, int(blocks)))
+
     def tie_info(self) -> dict:
         """Straddling ties of the top-k selections so far (psipm_tie_info)."""
         out = np.zeros(4, dtype=np.int64)

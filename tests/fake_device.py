@@ -70,6 +70,9 @@ class FakeDevice:
     def tie_info(self):
         return dict(straddles=0, tied=0, slots=0, selections=0)
 
+    def set_deterministic(self, on):
+        self.deterministic = bool(on)
+
     def get_theta(self):
         return self.theta.copy()
 
