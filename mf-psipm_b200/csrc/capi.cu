@@ -135,6 +135,8 @@ struct psipm_handle {
     DevBuf<int> frow_nch_d, ecnt_d, brow_nch_d, fcount_d, ecount_d, bcount_d;
     DevBuf<long long> frow_slot_d, eslot_off_d, uslot_d, brow_slot_d;
     int64_t nfslots = 0, neslots = 0, nbslots = 0;
+    std::vector<int> fdst_host;  // fdst of the current analysis (slot maps are built from it)
+    bool slots_ready = false;
     std::vector<int> solve_big_sn;        // supernodes with a transposed panel
     std::vector<int64_t> gt_off_host;
     DevBuf<long long> gt_off_d;
@@ -372,6 +374,84 @@ const float* a_values(psipm_handle* h, const float*) { return h->a_valf.p; }
 const double* weights(psipm_handle* h, const double*) { return h->w.p; }
 const float* weights(psipm_handle* h, const float*) { return h->wf.p; }
 
+// Slot maps of the deterministic apply, built on first use after each
+// symbolic analysis (handles that never ask for determinism pay nothing).
+void build_slot_maps(psipm_handle* h) {
+    const Symbolic& s = h->sym;
+    cudaStream_t st = h->stream;
+    const std::vector<int>& fdst = h->fdst_host;
+// slots of the fixed-order accumulation (kernels_pcg.cuh, slot_arrive):
+    //  forward: every GEMV task writes one partial per row of its 4-row group;
+    //  update rows: one slot per (child update row -> parent front row), in
+    //  ascending child and row order; backward: one partial per covering task
+    const int64_t nfront = std::max<int64_t>(1, s.sn_rowptr[s.ns]);
+    std::vector<int> frow_nch(nfront, 0), ecnt(nfront, 0), brow_nch(std::max<int64_t>(1, h->m), 0);
+    std::vector<long long> frow_slot(nfront, 0), eslot_off(nfront + 1, 0), brow_slot(std::max<int64_t>(1, h->m), 0);
+    std::vector<long long> uslot(std::max<int64_t>(1, s.uvec_off[s.ns]), 0);
+    int64_t nf = 0, nb = 0;
+    for (int sn = 0; sn < s.ns; ++sn) {
+        const int first = s.sn_first[sn], c = s.sn_first[sn + 1] - first;
+        const int64_t rb = s.sn_rowptr[sn];
+        const int r = (int)(s.sn_rowptr[sn + 1] - rb);
+        if (r <= kSmallRows && c <= 32) continue;  // fused: rows written directly
+        const int cch = (c + kApplyChunk - 1) / kApplyChunk;
+        for (int i0 = 0; i0 < r; i0 += kApplyRows) {
+            const int i1 = std::min(r, i0 + kApplyRows);
+            const int nch = (i1 - 1 < c) ? (i1 - 1) / kApplyChunk + 1 : cch;
+            for (int ii = i0; ii < i1; ++ii) {
+                frow_nch[rb + ii] = nch;
+                frow_slot[rb + ii] = nf;
+                nf += nch;
+            }
+        }
+        const int rch = (r + kApplyChunk - 1) / kApplyChunk;
+        for (int j0 = 0; j0 < c; j0 += kApplyRows) {
+            const int nch = rch - j0 / kApplyChunk;
+            for (int jj = j0; jj < std::min(c, j0 + kApplyRows); ++jj) {
+                brow_nch[first + jj] = nch;
+                brow_slot[first + jj] = nb;
+                nb += nch;
+            }
+        }
+    }
+    for (int64_t u = 0; u < s.uvec_off[s.ns]; ++u)
+        if (fdst[u] >= 0) ++ecnt[fdst[u]];
+    for (int64_t g = 0; g < nfront; ++g) eslot_off[g + 1] = eslot_off[g] + ecnt[g];
+    {
+        std::vector<long long> fill(eslot_off.begin(), eslot_off.end() - 1);
+        for (int64_t u = 0; u < s.uvec_off[s.ns]; ++u)  // children ascending, rows ascending
+            if (fdst[u] >= 0) uslot[u] = fill[fdst[u]]++;
+    }
+    h->nfslots = std::max<int64_t>(1, nf);
+    h->nbslots = std::max<int64_t>(1, nb);
+    h->neslots = std::max<int64_t>(1, eslot_off[nfront]);
+    h->frow_nch_d.upload(frow_nch, st);
+    h->frow_slot_d.upload(frow_slot, st);
+    h->ecnt_d.upload(ecnt, st);
+    h->eslot_off_d.upload(eslot_off, st);
+    h->uslot_d.upload(uslot, st);
+    h->brow_nch_d.upload(brow_nch, st);
+    h->brow_slot_d.upload(brow_slot, st);
+    h->fcount_d.zero(nfront, st);
+    h->ecount_d.zero(nfront, st);
+    h->bcount_d.zero(std::max<int64_t>(1, h->m), st);
+
+    h->slots_ready = true;
+}
+
+// A multifrontal workspace above this size is given back after every
+// factorisation (the PCG that follows does not use it); smaller ones stay
+// allocated for the next factorisation.
+constexpr int64_t kKeepWorkspaceBytes = int64_t(2) << 30;
+
+template <typename T>
+void release_workspace(FactorStore<T>& fs) {
+    if ((int64_t)((fs.update.n + fs.front.n) * sizeof(T)) > kKeepWorkspaceBytes) {
+        fs.update.release();
+        fs.front.release();
+    }
+}
+
 template <typename T, typename P = T>
 PcgArgs<T, P> pcg_args(psipm_handle* h) {
     const T* tag = nullptr;
@@ -400,6 +480,12 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
         pc.fown = h->fown_d.p;
         pc.fdst = h->fdst_d.p;
         pc.deterministic = h->deterministic ? 1 : 0;
+        if (h->deterministic) {
+            if (!h->slots_ready) build_slot_maps(h);
+            fs.fslots.reserve(h->nfslots);
+            fs.eslots.reserve(h->neslots);
+            fs.bslots.reserve(h->nbslots);
+        }
         pc.frow_nch = h->frow_nch_d.p;
         pc.frow_slot = h->frow_slot_d.p;
         pc.fcount = h->fcount_d.p;
@@ -624,61 +710,8 @@ void analyse(psipm_handle* h) {
         }
         h->fown_d.upload(fown, st);
         h->fdst_d.upload(fdst, st);
-        // slots of the fixed-order accumulation (kernels_pcg.cuh, slot_arrive):
-        //  forward: every GEMV task writes one partial per row of its 4-row group;
-        //  update rows: one slot per (child update row -> parent front row), in
-        //  ascending child and row order; backward: one partial per covering task
-        const int64_t nfront = std::max<int64_t>(1, s.sn_rowptr[s.ns]);
-        std::vector<int> frow_nch(nfront, 0), ecnt(nfront, 0), brow_nch(std::max<int64_t>(1, h->m), 0);
-        std::vector<long long> frow_slot(nfront, 0), eslot_off(nfront + 1, 0), brow_slot(std::max<int64_t>(1, h->m), 0);
-        std::vector<long long> uslot(std::max<int64_t>(1, s.uvec_off[s.ns]), 0);
-        int64_t nf = 0, nb = 0;
-        for (int sn = 0; sn < s.ns; ++sn) {
-            const int first = s.sn_first[sn], c = s.sn_first[sn + 1] - first;
-            const int64_t rb = s.sn_rowptr[sn];
-            const int r = (int)(s.sn_rowptr[sn + 1] - rb);
-            if (r <= kSmallRows && c <= 32) continue;  // fused: rows written directly
-            const int cch = (c + kApplyChunk - 1) / kApplyChunk;
-            for (int i0 = 0; i0 < r; i0 += kApplyRows) {
-                const int i1 = std::min(r, i0 + kApplyRows);
-                const int nch = (i1 - 1 < c) ? (i1 - 1) / kApplyChunk + 1 : cch;
-                for (int ii = i0; ii < i1; ++ii) {
-                    frow_nch[rb + ii] = nch;
-                    frow_slot[rb + ii] = nf;
-                    nf += nch;
-                }
-            }
-            const int rch = (r + kApplyChunk - 1) / kApplyChunk;
-            for (int j0 = 0; j0 < c; j0 += kApplyRows) {
-                const int nch = rch - j0 / kApplyChunk;
-                for (int jj = j0; jj < std::min(c, j0 + kApplyRows); ++jj) {
-                    brow_nch[first + jj] = nch;
-                    brow_slot[first + jj] = nb;
-                    nb += nch;
-                }
-            }
-        }
-        for (int64_t u = 0; u < s.uvec_off[s.ns]; ++u)
-            if (fdst[u] >= 0) ++ecnt[fdst[u]];
-        for (int64_t g = 0; g < nfront; ++g) eslot_off[g + 1] = eslot_off[g] + ecnt[g];
-        {
-            std::vector<long long> fill(eslot_off.begin(), eslot_off.end() - 1);
-            for (int64_t u = 0; u < s.uvec_off[s.ns]; ++u)  // children ascending, rows ascending
-                if (fdst[u] >= 0) uslot[u] = fill[fdst[u]]++;
-        }
-        h->nfslots = std::max<int64_t>(1, nf);
-        h->nbslots = std::max<int64_t>(1, nb);
-        h->neslots = std::max<int64_t>(1, eslot_off[nfront]);
-        h->frow_nch_d.upload(frow_nch, st);
-        h->frow_slot_d.upload(frow_slot, st);
-        h->ecnt_d.upload(ecnt, st);
-        h->eslot_off_d.upload(eslot_off, st);
-        h->uslot_d.upload(uslot, st);
-        h->brow_nch_d.upload(brow_nch, st);
-        h->brow_slot_d.upload(brow_slot, st);
-        h->fcount_d.zero(nfront, st);
-        h->ecount_d.zero(nfront, st);
-        h->bcount_d.zero(std::max<int64_t>(1, h->m), st);
+        h->fdst_host = std::move(fdst);
+        h->slots_ready = false;
     }
     // per level: fronts factored one per CTA (small) or by the multi-CTA path (big)
     h->small_ptr.assign(s.nlevels + 1, 0);
@@ -709,16 +742,10 @@ void analyse(psipm_handle* h) {
         fs.ms.reserve(std::max<int64_t>(1, s.nentries));
         fs.G.reserve(std::max<int64_t>(1, s.panel_total));
         fs.GT.reserve(std::max<int64_t>(1, s.panel_total));
-        fs.update.reserve(std::max<int64_t>(1, s.update_total));
-        fs.front.reserve(std::max<int64_t>(1, fmax_total));
         fs.xp.reserve(h->m);
         fs.yp.reserve(h->m);
         fs.dscp.reserve(h->m);
         fs.fvec.reserve(std::max<int64_t>(1, s.sn_rowptr[s.ns]));
-        fs.fslots.reserve(h->nfslots);
-        fs.eslots.reserve(h->neslots);
-        fs.bslots.reserve(h->nbslots);
-        fs.dinv.reserve((int64_t)(s.max_cols / kGB + 1) * kGB * kGB);  // D_J^T blocks of one big front
     };
     if (h->precision != PSIPM_FP64)
         reserve_factor(h->f32);
@@ -826,6 +853,11 @@ int factor_numeric(psipm_handle* h, double delta, int start_shift) {
     Symbolic& s = h->sym;
     cudaStream_t st = h->stream;
     FactorStore<T>& fs = fstore(h, tag);
+    // multifrontal workspace: update matrices, one level's fronts, the
+    // diagonal-block inverses of a big front
+    fs.update.reserve(std::max<int64_t>(1, s.update_total));
+    fs.front.reserve(std::max<int64_t>(1, h->front_total));
+    fs.dinv.reserve((int64_t)(s.max_cols / kGB + 1) * kGB * kGB);
     if (s.nentries)
         LAUNCH(h, k_assemble_entries<<<blocks_for(s.nentries, 256), 256, 0, st>>>(
                       s.nentries, h->s_ent_ptr.p, h->s_contrib_col.p, h->s_contrib_val.p, h->d_core.p, h->w.p,
@@ -871,8 +903,12 @@ int factor_numeric(psipm_handle* h, double delta, int start_shift) {
         int failed = 0;
         PSIPM_CUDA(cudaMemcpyAsync(&failed, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         PSIPM_CUDA(cudaStreamSynchronize(st));
-        if (!failed) return k;
+        if (!failed) {
+            release_workspace(fs);
+            return k;
+        }
     }
+    release_workspace(fs);
     return -1;
 }
 

@@ -366,8 +366,6 @@ class GpuStableActiveColumnPreconditioner:
             raise KKTSolveError(str(exc)) from exc
         self.stats["not_pd"] += used - start
         self._shift = SHIFTS[used]
-        if self.factor_hook is not None:
-            self.factor_hook(self, used)
         if used > 0:
             self.n_shifted += 1
         self.n_symbolic = int(info.symbolic_analyses)
@@ -378,6 +376,8 @@ class GpuStableActiveColumnPreconditioner:
         self._has_factor = True
         self.n_fact += 1
         self.t_fact += time.perf_counter() - t0
+        if self.factor_hook is not None:
+            self.factor_hook(self, used)
 
     def factorize(self, theta, delta) -> None:  # psipm_stable_preconditioner.py:397-432
         theta = theta if theta is RESIDENT else np.asarray(theta, dtype=float)
