@@ -232,6 +232,9 @@ int guarded(psipm_handle* h, F&& body) {
         }
         return PSIPM_OK;
     } catch (const Failure& f) {
+        // a failed allocation or launch also sets the runtime's last error; clear
+        // it so that it is not reported again by this handle's next launch check
+        (void)cudaGetLastError();
         return fail_code(h, f);
     } catch (const std::bad_alloc&) {
         h->err = "host allocation failed";
@@ -563,7 +566,17 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
     return a;
 }
 
-size_t pcg_smem() { return (size_t)kPcgWarps * kStageChunk * sizeof(double); }  // covers float too
+size_t pcg_smem() { return (size_t)kPcgWarps * kWarpSmemBytes; }  // covers float too
+
+// the persistent kernels take more than the default 48 KB of dynamic shared memory
+void set_pcg_smem_attributes() {
+    const int bytes = (int)pcg_smem();
+    const void* fns[] = {(const void*)k_pcg<double, double>, (const void*)k_pcg<double, float>,
+                         (const void*)k_pcg<float, float>,  (const void*)k_apply<double, double>,
+                         (const void*)k_apply<double, float>, (const void*)k_matvec<double, double>};
+    for (const void* fn : fns)
+        PSIPM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
 
 void launch_coop(psipm_handle* h, const void* fn, void** args) {
     prepare_barrier(h);
@@ -576,6 +589,7 @@ void launch_coop(psipm_handle* h, const void* fn, void** args) {
 // symbolic analysis of the current core and upload of its arrays
 void analyse(psipm_handle* h) {
     auto t0 = std::chrono::steady_clock::now();
+    h->have_symbolic = false;  // until the new analysis and its device arrays are complete
     read_thresholds();
     SymbolicOptions opt;
     Symbolic S;
@@ -1186,16 +1200,7 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
         PSIPM_CUDA(cudaGetDeviceProperties(&prop, device));
         h->num_sms = prop.multiProcessorCount;
         require(prop.cooperativeLaunch, PSIPM_ERR_UNSUPPORTED, "device lacks cooperative launch");
-        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)pcg_smem()));
-        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)pcg_smem()));
-        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)pcg_smem()));
-        PSIPM_CUDA(cudaFuncSetAttribute(k_apply<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)pcg_smem()));
-        PSIPM_CUDA(cudaFuncSetAttribute(k_pcg<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)pcg_smem()));
+        set_pcg_smem_attributes();
         PSIPM_CUDA(cudaFuncSetAttribute(k_trsm_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)(2 * kNB * (kNB + 1) * sizeof(float))));
         PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1217,7 +1222,8 @@ int psipm_create(int64_t m, int64_t n, int64_t nnz, const int64_t* colptr, const
         PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_apply<double, double>, kPcgThreads,
                                                                  pcg_smem()));
         int per_sm3 = 0;
-        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_matvec<double, double>, kPcgThreads, 0));
+        PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_matvec<double, double>, kPcgThreads,
+                                                                 pcg_smem()));
         int per_sm4 = 0;
         PSIPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, k_pcg<float, float>, kPcgThreads, pcg_smem()));
         int per_sm5 = 0;
@@ -1469,6 +1475,7 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
     int status = guarded(h, [&]() {
         require(h->have_theta, PSIPM_ERR_STATE, "factor before set_theta");
         require(!h->tree_mode, PSIPM_ERR_STATE, "the handle uses the tree preconditioner (psipm_tree_factor)");
+        h->have_factor = false;  // until this factorisation succeeds (a failed one leaves no factor)
         if (h->core_dirty || !h->have_symbolic) analyse(h);
         h->delta = delta;
         Symbolic& s = h->sym;

@@ -245,6 +245,7 @@ class GpuStableActiveColumnPreconditioner:
         self.device_seconds = 0.0
         self.core_history = []
         self.tie_straddles = 0
+        self.memory_caps = 0  # core targets lowered because a factor did not fit in device memory
         # learned selector (no counterpart in the reference): a SelectorModel that
         # re-scores the candidates before the rule's refresh; a learned core that
         # turns out poor by the rule's own signals suspends it for
@@ -359,6 +360,16 @@ class GpuStableActiveColumnPreconditioner:
             used, info = self.dev.factor(float(delta), start)
         except DeviceError as exc:
             self.t_fact += time.perf_counter() - t0
+            if exc.status == _lib.ERR_MEMORY and self.core.size > self.mandatory.size:
+                # the factor of this core does not fit in device memory: cap the
+                # core below its size and refresh at the next factorisation
+                cap = max(int(self.mandatory.size), int(0.8 * self.core.size))
+                self.max_core_target = min(self.max_core_target, cap)
+                self.core_target = min(self.core_target, cap)
+                self._initialized = False
+                self._has_factor = False
+                self.memory_caps += 1
+                raise KKTSolveError(f"the factor does not fit in device memory ({exc})") from exc
             if exc.status == _lib.ERR_NOT_PD:
                 self.stats["not_pd"] += 8 - start
                 self._has_factor = False
