@@ -445,7 +445,7 @@ void build_slot_maps(psipm_handle* h) {
 // A multifrontal workspace above this size is given back after every
 // factorisation (the PCG that follows does not use it); smaller ones stay
 // allocated for the next factorisation.
-constexpr int64_t kKeepWorkspaceBytes = int64_t(2) << 30;
+constexpr int64_t kKeepWorkspaceBytes = int64_t(16) << 30;
 
 template <typename T>
 void release_workspace(FactorStore<T>& fs) {
@@ -566,7 +566,7 @@ PcgArgs<T, P> pcg_args(psipm_handle* h) {
     return a;
 }
 
-size_t pcg_smem() { return (size_t)kPcgWarps * kWarpSmemBytes; }  // covers float too
+size_t pcg_smem() { return (size_t)kPcgWarps * kStageChunk * sizeof(double); }  // covers float too
 
 // the persistent kernels take more than the default 48 KB of dynamic shared memory
 void set_pcg_smem_attributes() {

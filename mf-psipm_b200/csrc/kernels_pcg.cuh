@@ -430,65 +430,14 @@ __device__ __forceinline__ void deliver_update(const PrecLayout<P>& pc, long lon
         pc.fvec[e] = slot_sum(pc.eslots, pc.eslot_off[e], ne, __ldcg(pc.fvec + e));
 }
 
-// ---- asynchronous staging of a task's panel tile ------------------------------
-// Each warp owns a two-stage ring of kApplyRows x kApplyChunk panel entries in
-// shared memory.  While it works on one GEMV task from one stage, cp.async
-// copies the next task's tile into the other stage, so the panel loads of the
-// next task are in flight during this task's arithmetic, reduction and
-// epilogue instead of after them.  Copies are element-sized (panel rows have
-// no 16-byte alignment); every copied address is clamped inside its row.
-constexpr int kTile = kApplyRows * kApplyChunk;
-// per-warp shared memory of the apply: staging of a small supernode, the
-// two-stage panel ring and the two stages' task records (sized for FP64)
-constexpr int kRingBytes = 8 * (kStageChunk + 2 * kTile);
-constexpr int kWarpSmemBytes = kRingBytes + 2 * 48;
-
-template <typename P>
-__device__ __forceinline__ void cp_async_elem(P* smem, const P* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    if constexpr (sizeof(P) == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// rows i0 + k (clamped to the task's rows) x columns j0 + lane + 32 q (clamped to c)
-template <typename P>
-__device__ __forceinline__ void stage_forward(const PrecLayout<P>& pc, const FwdTask& t, P* S) {
-    const int lane = threadIdx.x & 31;
-    const P* G = pc.G + t.g;
-#pragma unroll
-    for (int k = 0; k < kApplyRows; ++k) {
-        const P* g = G + (long long)min(k, t.i1 - t.i0 - 1) * t.c;
-#pragma unroll
-        for (int q = 0; q < kLaneCols; ++q)
-            cp_async_elem(S + k * kApplyChunk + lane + 32 * q, g + min(t.j0 + lane + 32 * q, t.c - 1));
-    }
-}
-// GT rows j0 + k (clamped) x front rows i0 + lane + 32 q (clamped to r)
-template <typename P>
-__device__ __forceinline__ void stage_backward(const PrecLayout<P>& pc, const BwdTask& t, P* S) {
-    const int lane = threadIdx.x & 31;
-    const P* GT = pc.GT + t.g;
-#pragma unroll
-    for (int k = 0; k < kApplyRows; ++k) {
-        const P* g = GT + (long long)min(k, t.j1 - t.j0 - 1) * t.r;
-#pragma unroll
-        for (int q = 0; q < kLaneCols; ++q)
-            cp_async_elem(S + k * kApplyChunk + lane + 32 * q, g + min(t.i0 + lane + 32 * q, t.r - 1));
-    }
-}
-
 // forward task: rows [i0, i1) (at most four) of G against f[j0, j0 + kApplyChunk).
 // Every lane loads a clamped in-row index and masks the product, so the
 // sixteen loads carry no branches and issue together.
 template <typename P>
-__device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t, const P* S) {
+__device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t) {
     const int lane = threadIdx.x & 31;
     const int c = t.c, i0 = t.i0, i1 = t.i1, j0 = t.j0;
+    const P* __restrict__ G = pc.G + t.g;
     const P* f = pc.fvec + t.f;
     const int j1 = min(c, j0 + kApplyChunk);
     const int ii = i0 + lane;  // the row lane k < 4 finishes
@@ -505,11 +454,12 @@ __device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t, con
         const int row = i0 + k;
         // G_top is lower triangular; rows past i1 contribute nothing
         const int jend = row < i1 ? (row < c ? min(j1, row + 1) : j1) : j0;
+        const P* __restrict__ g = G + (long long)min(k, i1 - i0 - 1) * c;
         P acc = 0;
 #pragma unroll
         for (int q = 0; q < kLaneCols; ++q) {
             const int j = j0 + lane + 32 * q;
-            const P gv = S[k * kApplyChunk + lane + 32 * q];
+            const P gv = g[min(j, c - 1)];
             acc += j < jend ? gv * fr[q] : (P)0;
         }
         d[k] = acc;
@@ -537,10 +487,11 @@ __device__ void prec_forward_gemv(const PrecLayout<P>& pc, const FwdTask& t, con
 
 // backward task: GT rows [j0, j1) (at most four) against v[i0, i0 + kApplyChunk)
 template <typename P>
-__device__ void prec_backward_gemv(const PrecLayout<P>& pc, const BwdTask& t, const P* S) {
+__device__ void prec_backward_gemv(const PrecLayout<P>& pc, const BwdTask& t) {
     const int lane = threadIdx.x & 31;
     const int c = t.c, r = t.r, j0 = t.j0, j1 = t.j1, i0 = t.i0;
     const int i1 = min(r, i0 + kApplyChunk);
+    const P* __restrict__ GT = pc.GT + t.g;
     P vr[kLaneCols];
 #pragma unroll
     for (int q = 0; q < kLaneCols; ++q) {
@@ -552,11 +503,12 @@ __device__ void prec_backward_gemv(const PrecLayout<P>& pc, const BwdTask& t, co
     for (int k = 0; k < 4; ++k) {
         const int jj = j0 + k;
         const int ibeg = jj < j1 ? max(i0, jj) : i1;  // G[i, j] = 0 for i < j
+        const P* __restrict__ g = GT + (long long)min(k, j1 - j0 - 1) * r;
         P acc = 0;
 #pragma unroll
         for (int q = 0; q < kLaneCols; ++q) {
             const int i = i0 + lane + 32 * q;
-            const P gv = S[k * kApplyChunk + lane + 32 * q];
+            const P gv = g[min(i, r - 1)];
             acc += (i >= ibeg && i < i1) ? gv * vr[q] : (P)0;
         }
         d[k] = acc;
@@ -714,13 +666,9 @@ __device__ void prec_tree(const TreeLayout& t, const IT* in, IT* out, double& ac
 
 // z = P^{-1} in; acc_rz += in . z.  Ends without a barrier (the caller's
 // reduction provides it).
-// fs: the warp's staging buffer for small supernodes (kStageChunk entries),
-// followed in shared memory by its two-stage panel ring (2 kTile entries) and,
-// kRingBytes from fs, the two stages' task records.
 template <typename P, typename IT>
 __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, double& acc_rz, P* fs,
                            const GridBarrier& grid) {
-    P* ring = fs + kStageChunk;
     if (pc.tree.nlevels > 0) {
         prec_tree(pc.tree, in, out, acc_rz, grid);
         return;
@@ -752,76 +700,29 @@ __device__ void prec_apply(const PrecLayout<P>& pc, const IT* in, IT* out, doubl
     }
     grid.sync();
     mark();
-    // Tasks of a level: fused small supernodes (s >= 0) or 2-D GEMV tasks whose
-    // panel tiles go through the warp's two-stage ring (the next task's tile is
-    // copied while this one is computed).  The next record is loaded one task
-    // ahead as well.
-    const bool lead = (threadIdx.x & 31) == 0;
+    // task kind (int4.w for fused tasks is -1): fused small supernode or 2-D GEMV
     for (int lev = 0; lev < pc.nlevels; ++lev) {
-        const int end = pc.fwd_ptr[lev + 1];
-        FwdTask* rec = reinterpret_cast<FwdTask*>(reinterpret_cast<unsigned char*>(fs) + kRingBytes);
-        int tk = pc.fwd_ptr[lev] + gwarp;
-        int stage = 0;
-        if (tk < end) {
-            const FwdTask t = pc.fwd_tasks[tk];
-            if (t.s < 0) stage_forward(pc, t, ring);
-            if (lead) rec[0] = t;
-        }
-        cp_async_commit();
-        while (tk < end) {
-            const int nk = tk + nwarps;
-            if (nk < end) {  // the next record and tile, while this task runs
-                const FwdTask t = pc.fwd_tasks[nk];
-                if (t.s < 0) stage_forward(pc, t, ring + (stage ^ 1) * kTile);
-                if (lead) rec[stage ^ 1] = t;
-            }
-            cp_async_commit();
-            cp_async_wait_prior();  // this task's tile has landed
-            __syncwarp();
-            const FwdTask cur = rec[stage];
-            if (cur.s >= 0)
-                prec_forward_small(pc, cur.s, fs);
+        for (int tk = pc.fwd_ptr[lev] + gwarp; tk < pc.fwd_ptr[lev + 1]; tk += nwarps) {
+            // the record of this warp's next task is pulled into L2 meanwhile
+            if ((threadIdx.x & 31) == 0 && tk + nwarps < pc.fwd_ptr[lev + 1]) prefetch_l2(pc.fwd_tasks + tk + nwarps);
+            const FwdTask task = pc.fwd_tasks[tk];
+            if (task.s >= 0)
+                prec_forward_small(pc, task.s, fs);
             else
-                prec_forward_gemv(pc, cur, ring + stage * kTile);
-            __syncwarp();  // the stage is free for the task after next
-            tk = nk;
-            stage ^= 1;
+                prec_forward_gemv(pc, task);
         }
-        cp_async_wait_all();
         grid.sync();
         mark();
     }
     for (int lev = pc.nlevels - 1; lev >= 0; --lev) {
-        const int end = pc.bwd_ptr[lev + 1];
-        BwdTask* rec = reinterpret_cast<BwdTask*>(reinterpret_cast<unsigned char*>(fs) + kRingBytes);
-        int tk = pc.bwd_ptr[lev] + gwarp;
-        int stage = 0;
-        if (tk < end) {
-            const BwdTask t = pc.bwd_tasks[tk];
-            if (t.s < 0) stage_backward(pc, t, ring);
-            if (lead) rec[0] = t;
-        }
-        cp_async_commit();
-        while (tk < end) {
-            const int nk = tk + nwarps;
-            if (nk < end) {
-                const BwdTask t = pc.bwd_tasks[nk];
-                if (t.s < 0) stage_backward(pc, t, ring + (stage ^ 1) * kTile);
-                if (lead) rec[stage ^ 1] = t;
-            }
-            cp_async_commit();
-            cp_async_wait_prior();
-            __syncwarp();
-            const BwdTask cur = rec[stage];
-            if (cur.s >= 0)
-                prec_backward_small(pc, cur.s, fs);
+        for (int tk = pc.bwd_ptr[lev] + gwarp; tk < pc.bwd_ptr[lev + 1]; tk += nwarps) {
+            if ((threadIdx.x & 31) == 0 && tk + nwarps < pc.bwd_ptr[lev + 1]) prefetch_l2(pc.bwd_tasks + tk + nwarps);
+            const BwdTask task = pc.bwd_tasks[tk];
+            if (task.s >= 0)
+                prec_backward_small(pc, task.s, fs);
             else
-                prec_backward_gemv(pc, cur, ring + stage * kTile);
-            __syncwarp();
-            tk = nk;
-            stage ^= 1;
+                prec_backward_gemv(pc, task);
         }
-        cp_async_wait_all();
         grid.sync();
         mark();
     }
@@ -854,7 +755,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs<T, P> a) {
     const GridBarrier grid = a.gb;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double scratch[kPcgWarps + 1];
-    P* fs = reinterpret_cast<P*>(smem_raw + (threadIdx.x >> 5) * kWarpSmemBytes);
+    P* fs = reinterpret_cast<P*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
     const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
@@ -1124,7 +1025,7 @@ template <typename T, typename P>
 __global__ void __launch_bounds__(kPcgThreads, 3) k_apply(PcgArgs<T, P> a, const T* in, T* out) {
     const GridBarrier grid = a.gb;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    P* fs = reinterpret_cast<P*>(smem_raw + (threadIdx.x >> 5) * kWarpSmemBytes);
+    P* fs = reinterpret_cast<P*>(smem_raw) + (threadIdx.x >> 5) * kStageChunk;
     double dummy = 0.0;
     prec_apply(a.pc, in, out, dummy, fs, grid);
 }

@@ -228,3 +228,35 @@ def test_resident_predictor_corrector_variants(pc, golden):
     assert sol.status == "optimal"
     ref = float(g["obj"])
     assert abs(sol.obj - ref) <= 1e-7 * abs(ref)
+
+
+@pytest.mark.parametrize("family", ["random", "grid", "cover"])
+def test_device_starting_point_matches_the_oracle(family):
+    """psipm_ipm_start against the oracle's arithmetic of the reference's start
+    (psipm_active_pool.py:4190-4240) applied to the same two projections."""
+    from oracle import ipm as OI
+    from psipm_b200 import synthetic
+    from psipm_b200.device import NormalEquationsDevice
+
+    lp = {"random": lambda: synthetic.random_lp(300, 900, seed=3),
+          "grid": lambda: synthetic.grid_network(12, 15, seed=4),
+          "cover": lambda: synthetic.set_cover(200, 5000, seed=5)}[family]()
+    m, n = lp.A.shape
+    dev = NormalEquationsDevice(lp.A)
+    try:
+        dev.ipm_load(lp.c, lp.b, lp.u, lp.pos, lp.box)
+        dev.set_theta(np.ones(n), 1.0)
+        dev.set_core(dev.candidates[: min(dev.candidates.size, 2 * m)])
+        dev.factor(1.0, 0)
+        for which in (0, 1):
+            finite, res = dev.ipm_start_solve(which, 1e-12, 500)
+            assert finite and res.ok
+        x0, y0, _, _ = dev.ipm_get(0)
+        dev.ipm_start(True)
+        x, y, z, w = dev.ipm_get(0)
+        ibox = slice(None) if lp.box.all() else np.flatnonzero(lp.box)
+        xr, yr, zr, wr = OI.start_from_projections(lp.A.T.tocsr(), lp.c, lp.u, lp, ibox, x0.copy(), y0.copy())
+        for a, b_, name in ((x, xr, "x"), (y, yr, "y"), (z, zr, "z"), (w, wr, "w")):
+            assert np.allclose(a, b_, rtol=1e-11, atol=1e-11 * max(1.0, np.abs(b_).max())), name
+    finally:
+        dev.close()
