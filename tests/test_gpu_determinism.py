@@ -87,3 +87,40 @@ def test_refresh_and_refactor_decisions_follow_the_reference(name, golden):
         assert abs(solver.n_fact - int(g["n_fact"])) <= 2
     finally:
         solver.close()
+
+
+@pytest.mark.parametrize("family", ["grid", "cover_small", "cover_wide"])
+def test_fixed_order_apply_matches_the_atomic_apply(family):
+    """The fixed-order accumulation computes the same preconditioner as the
+    default atomic accumulation: the two applies differ only in the order of
+    their additions (to 1e-13 relative on these factors), and the fixed order
+    repeats its bits."""
+    from psipm_b200 import synthetic
+    from psipm_b200.device import NormalEquationsDevice
+
+    lp = {"grid": lambda: synthetic.grid_network(60, 80, seed=5),
+          "cover_small": lambda: synthetic.set_cover(400, 20_000, seed=2001),
+          "cover_wide": lambda: synthetic.set_cover(1500, 60_000, seed=2002)}[family]()
+    m = lp.A.shape[0]
+    dev = NormalEquationsDevice(lp.A)
+    try:
+        rng = np.random.default_rng(3)
+        theta = np.exp(rng.uniform(-6, 6, lp.A.shape[1]))
+        delta = 1e-8
+        dev.set_theta(theta, delta)
+        core = np.sort(rng.choice(dev.candidates, min(dev.candidates.size, 2 * m), replace=False))
+        dev.set_core(core)
+        dev.factor(delta, 0)
+        r = rng.standard_normal(m)
+        z_atomic = dev.apply(r)
+        dev.set_deterministic(True)
+        z_fixed = dev.apply(r)
+        assert np.array_equal(dev.apply(r), z_fixed)
+        dev.set_deterministic(False)
+        z_again = dev.apply(r)
+        scale = np.linalg.norm(z_atomic)
+        assert np.isfinite(z_fixed).all()
+        assert np.linalg.norm(z_fixed - z_atomic) <= 1e-13 * scale
+        assert np.linalg.norm(z_again - z_atomic) <= 1e-13 * scale
+    finally:
+        dev.close()
