@@ -147,6 +147,16 @@ int psipm_set_deterministic(psipm_handle* h, int32_t on);
  * own streams each take a share of the GPU this way (psipm_b200.batch).  Not
  * with extracted dense columns (PSIPM_ERR_STATE). */
 int psipm_set_grid(psipm_handle* h, int32_t blocks);
+/* Arithmetic of the FP32 factor's large fronts (PSIPM_FP32_REFINED and
+ * PSIPM_FP32_PRECOND handles; the FP64 factor always runs on the CUDA cores):
+ * `passes` 3 (the default) factors them in panels of 256 columns whose
+ * trailing updates run on the tensor cores as 3xTF32 products (hi*hi + hi*lo
+ * + lo*hi of a TF32 head and its FP32 remainder: FP32-level products, FP32
+ * accumulation); 1 uses the TF32 heads alone; 0 keeps the CUDA-core blocked
+ * kernels.  The reference factors with CHOLMOD in FP64
+ * (psipm_active_pool.py:839-897); this switch has no counterpart there.
+ * Takes effect at the next psipm_factor. */
+int psipm_set_factor_tc(psipm_handle* h, int32_t passes);
 /* Straddling ties of the top-k selections (psipm_refresh_core, psipm_top_k).
  * The reference selects with np.argpartition (psipm_stable_preconditioner.py:
  * 97-110), whose pick among equal scores that straddle the cut depends on
@@ -342,6 +352,13 @@ int psipm_timer_stop(psipm_handle* h, double* seconds);
  * launch. */
 int psipm_debug_barrier_timeout(psipm_handle* h, int32_t count, int32_t polls, int32_t skip_block,
                                 double* seconds);
+/* Test hook of the tensor-core trailing update alone, on GPU `device`:
+ * f_out = f_in (column-major r x r, FP32) with
+ *   F[i, j] -= sum_{k < kb} F[i, k0 + k] F[j, k0 + k]  for k0 + kb <= j <= i < r, j < jend,
+ * computed by the kernel the FP32 factor uses (passes 3 or 1 as in
+ * psipm_set_factor_tc).  Host buffers; no handle. */
+int psipm_debug_syrk_tc(int32_t device, int32_t r, int32_t k0, int32_t kb, int32_t jend, int32_t passes,
+                        const float* f_in, float* f_out);
 /* Shape of the current symbolic factor by height level (out[8 * l + .] for
  * l < min(cap, *nlevels)): {supernodes, fused single-warp supernodes,
  * supernodes cut into GEMV tasks, forward tasks, backward tasks,

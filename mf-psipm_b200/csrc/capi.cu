@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "factor_tc.h"
 #include "kernels_factor.cuh"
 #include "kernels_ipm.cuh"
 #include "kernels_mlp.cuh"
@@ -88,6 +89,7 @@ struct psipm_handle {
     int coop_blocks = 0;
     int coop_max = 0;  // the largest co-resident grid of the persistent kernels
     bool deterministic = false;  // fixed-order accumulation in the preconditioner apply
+    int factor_tc = 3;           // FP32 big fronts: tensor-core updates (3 = 3xTF32, 1 = TF32, 0 = CUDA cores)
 
     // A in CSC on the host (needed by the symbolic analysis)
     std::vector<int64_t> colptr;
@@ -805,6 +807,9 @@ void compute_weights(psipm_handle* h) {
 }
 
 
+// Columns per panel of the FP32 tensor-core path: the trailing update's K.
+constexpr int kTcPanel = 256;
+
 // one large front by the multi-CTA blocked path (kernels_factor.cuh)
 template <typename T>
 void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
@@ -829,14 +834,42 @@ void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
     }
     const size_t trsm_smem = 2 * kNB * (kNB + 1) * sizeof(T);
     const size_t syrk_smem = 2 * kNB * (kNB + 1) * sizeof(T);
-    for (int k0 = 0; k0 < c; k0 += kNB) {
-        const int kb = std::min(kNB, c - k0);
+    // Cholesky of the diagonal block at k0 and the rows below it
+    auto panel_step = [&](int k0, int kb) {
         LAUNCH(h, k_potrf_diag<T><<<1, 256, 0, st>>>(F, r, k0, kb, fa.fail));
         const int rows = r - k0 - kb;
-        if (rows <= 0) continue;
-        LAUNCH(h, k_trsm_panel<T><<<blocks_for(rows, kTrsmRows), kTrsmRows, trsm_smem, st>>>(F, r, k0, kb));
-        const int ntile = (rows + 63) / 64;
-        LAUNCH(h, k_syrk_update<T><<<ntile * (ntile + 1) / 2, 256, syrk_smem, st>>>(F, r, k0, kb, ntile));
+        if (rows > 0)
+            LAUNCH(h, k_trsm_panel<T><<<blocks_for(rows, kTrsmRows), kTrsmRows, trsm_smem, st>>>(F, r, k0, kb));
+        return rows;
+    };
+    bool tensor_cores = false;
+    if constexpr (std::is_same<T, float>::value) tensor_cores = h->factor_tc > 0;
+    if (!tensor_cores) {
+        for (int k0 = 0; k0 < c; k0 += kNB) {
+            const int kb = std::min(kNB, c - k0);
+            const int rows = panel_step(k0, kb);
+            if (rows <= 0) continue;
+            const int ntile = (rows + 63) / 64;
+            LAUNCH(h, k_syrk_update<T><<<ntile * (ntile + 1) / 2, 256, syrk_smem, st>>>(F, r, k0, kb, ntile));
+        }
+    } else if constexpr (std::is_same<T, float>::value) {
+        // two-level blocking: panels of kTcPanel columns factored by kNB-wide
+        // steps whose updates stay inside the panel, then one tensor-core
+        // update of the whole trailing matrix with K = the panel width
+        for (int kp = 0; kp < c; kp += kTcPanel) {
+            const int kpe = std::min(c, kp + kTcPanel);
+            for (int k0 = kp; k0 < kpe; k0 += kNB) {
+                const int kb = std::min(kNB, kpe - k0);
+                if (panel_step(k0, kb) > 0 && k0 + kb < kpe) {
+                    syrk_update_tc(F, r, k0, kb, kpe, h->factor_tc, fa.fail, st);
+                    ++h->launches;
+                }
+            }
+            if (kpe < r) {
+                syrk_update_tc(F, r, kp, kpe - kp, r, h->factor_tc, fa.fail, st);
+                ++h->launches;
+            }
+        }
     }
     if (r > c) {
         const long long n2 = (long long)(r - c) * (r - c);
@@ -917,6 +950,10 @@ int factor_numeric(psipm_handle* h, double delta, int start_shift) {
         int failed = 0;
         PSIPM_CUDA(cudaMemcpyAsync(&failed, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         PSIPM_CUDA(cudaStreamSynchronize(st));
+        if (failed & kTcErrWait) {
+            release_workspace(fs);
+            throw Failure(PSIPM_ERR_CUDA, "tensor-core front update: completion wait expired");
+        }
         if (!failed) {
             release_workspace(fs);
             return k;
@@ -1442,6 +1479,12 @@ int psipm_set_deterministic(psipm_handle* h, int32_t on) {
     return PSIPM_OK;
 }
 
+int psipm_set_factor_tc(psipm_handle* h, int32_t passes) {
+    if (!h || (passes != 0 && passes != 1 && passes != 3)) return PSIPM_ERR_ARGUMENT;
+    h->factor_tc = passes;
+    return PSIPM_OK;
+}
+
 int psipm_set_grid(psipm_handle* h, int32_t blocks) {
     if (!h || blocks < 0) return PSIPM_ERR_ARGUMENT;
     if (h->lr_ready || !h->lr_cols.empty()) return PSIPM_ERR_STATE;  // lr_part is sized for the grid
@@ -1960,6 +2003,38 @@ int psipm_debug_barrier_timeout(psipm_handle* h, int32_t count, int32_t polls, i
         PSIPM_CUDA(cudaStreamSynchronize(h->stream));
         *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     });
+}
+
+int psipm_debug_syrk_tc(int32_t device, int32_t r, int32_t k0, int32_t kb, int32_t jend, int32_t passes,
+                        const float* f_in, float* f_out) {
+    if (r <= 0 || k0 < 0 || kb <= 0 || k0 + kb > r || jend > r || (passes != 1 && passes != 3) || !f_in ||
+        !f_out)
+        return PSIPM_ERR_ARGUMENT;
+    try {
+        PSIPM_CUDA(cudaSetDevice(device));
+        cudaStream_t st;
+        PSIPM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamDestroy(s); }
+        } guard{st};
+        const size_t bytes = (size_t)r * r * sizeof(float);
+        DevBuf<float> F;
+        DevBuf<int> err;
+        F.upload(f_in, (size_t)r * r, st);
+        err.zero(1, st);
+        syrk_update_tc(F.p, r, k0, kb, jend, passes, err.p, st);
+        int e = 0;
+        PSIPM_CUDA(cudaMemcpyAsync(f_out, F.p, bytes, cudaMemcpyDeviceToHost, st));
+        PSIPM_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PSIPM_CUDA(cudaStreamSynchronize(st));
+        return e ? PSIPM_ERR_TIMEOUT : PSIPM_OK;
+    } catch (const Failure& f) {
+        (void)cudaGetLastError();
+        return f.code;
+    } catch (...) {
+        return PSIPM_ERR_CUDA;
+    }
 }
 
 int psipm_debug_levels(const psipm_handle* h, int64_t* out, int32_t cap, int32_t* nlevels) {

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kFactorThreads) k_factor_level(FactorArgs<T> a
         }
         __syncthreads();
     }
-    if (tid == 0 && bad) atomicExch(a.fail, 1);
+    if (tid == 0 && bad) atomicOr(a.fail, 1);
     // update matrix: F[c:r, c:r] (column-major rc x rc)
     const int rc = r - c;
     if (rc > 0) {
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ F, int r, in
         const int i = q % kb, j = q / kb;
         if (i >= j) F[(long long)(k0 + j) * r + (k0 + i)] = D[i][j];
     }
-    if (tid == 0 && bad) atomicExch(fail, 1);
+    if (tid == 0 && bad) atomicOr(fail, 1);
 }
 
 // panel: F[i, k0:k0+kb] <- F[i, k0:k0+kb] L_kk^{-T} for rows i >= k0+kb

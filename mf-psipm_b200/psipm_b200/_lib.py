@@ -108,6 +108,7 @@ SIGNATURES = {
     "psipm_tie_info": (_I32, [_P, _P]),
     "psipm_set_grid": (_I32, [_P, _I32]),
     "psipm_set_deterministic": (_I32, [_P, _I32]),
+    "psipm_set_factor_tc": (_I32, [_P, _I32]),
     "psipm_top_k": (_I32, [_P, _P, _I64, _P, _I64, _P, _P]),
     "psipm_factor": (_I32, [_P, _D, _I32, _P, _P]),
     "psipm_apply": (_I32, [_P, _P, _P]),
@@ -123,6 +124,7 @@ SIGNATURES = {
     "psipm_debug_apply_trace": (_I32, [_P, _P, _P, _P, _I32, _P, _P]),
     "psipm_timer_stop": (_I32, [_P, _P]),
     "psipm_debug_barrier_timeout": (_I32, [_P, _I32, _I32, _I32, _P]),
+    "psipm_debug_syrk_tc": (_I32, [_I32, _I32, _I32, _I32, _I32, _I32, _P, _P]),
     "psipm_debug_levels": (_I32, [_P, _P, _I32, _P]),
     "psipm_ipm_load": (_I32, [_P, _P, _P, _P, _P, _P]),
     "psipm_ipm_put": (_I32, [_P, _I32, _P, _P, _P, _P]),

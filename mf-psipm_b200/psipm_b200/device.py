@@ -198,6 +198,11 @@ class NormalEquationsDevice:
         """Fixed-order accumulation in the preconditioner apply (psipm_set_deterministic)."""
         self._check(self.lib.psipm_set_deterministic(self.h, int(bool(on))))
 
+    def set_factor_tc(self, passes: int) -> None:
+        """FP32 big fronts on the tensor cores: 3 (3xTF32, default), 1 (TF32) or
+        0 (CUDA cores) (psipm_set_factor_tc)."""
+        self._check(self.lib.psipm_set_factor_tc(self.h, int(passes)))
+
     def set_grid(self, blocks: int) -> None:
         """Blocks of this handle's persistent kernels (0: the full co-resident grid)."""
         self._check(self.lib.psipm_set_grid(self.h, int(blocks)))

@@ -129,7 +129,8 @@ class GpuStableActiveColumnPreconditioner:
                  adaptive_refresh_row_threshold=20_000, order="best", refine=2, refine_tol=1e-10,
                  fail_tol=1e-6, extract_low_rank=True, low_rank_max_columns=8, low_rank_min_nnz=1024,
                  low_rank_clique_ratio=2.0, device=0, precision=_lib.FP64, dev=None, selector=None,
-                 selector_patience=2, selector_shift=True, selector_window=0.0, deterministic=False):
+                 selector_patience=2, selector_shift=True, selector_window=0.0, deterministic=False,
+                 factor_tc=3):
         if core_factor <= 0.0:
             raise ValueError("core_factor must be positive")
         if max_core_factor < core_factor:
@@ -164,6 +165,8 @@ class GpuStableActiveColumnPreconditioner:
         self.precision = precision
         if deterministic:  # bit-repeatable runs (slower applies)
             self.dev.set_deterministic(True)
+        if factor_tc != 3:  # FP32 big fronts: 3xTF32 tensor cores (3, the default), TF32 (1), CUDA cores (0)
+            self.dev.set_factor_tc(int(factor_tc))
         if self.low_rank_columns.size:
             # the factor leaves these columns out and corrects for them by
             # Woodbury (psipm_active_pool.py:786-798, 906-956)

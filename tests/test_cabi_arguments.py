@@ -29,7 +29,7 @@ def lib():
 
 def test_null_handle_is_rejected_by_every_entry_point(lib):
     skip = {"psipm_create", "psipm_normal_matvec_static", "psipm_mlp_forward_dev", "psipm_mlp_grad_dev",
-            "psipm_mlp_adam_dev"}
+            "psipm_mlp_adam_dev", "psipm_debug_syrk_tc"}
     checked = 0
     for name, (restype, argtypes) in _lib.SIGNATURES.items():
         if name in skip or not argtypes or argtypes[0] is not P:
@@ -45,6 +45,18 @@ def test_null_handle_is_rejected_by_every_entry_point(lib):
             assert out == _lib.ERR_ARGUMENT, name
         checked += 1
     assert checked == len(_lib.SIGNATURES) - len(skip)
+
+
+def test_tensor_core_hooks_reject_bad_arguments(lib):
+    f = lib.psipm_debug_syrk_tc
+    buf = (ctypes.c_float * 16)()
+    p = ctypes.cast(buf, P)
+    good = [0, 4, 0, 2, 4, 3, p, p]
+    for k, bad in ((1, 0), (2, -1), (3, 0), (3, 5), (4, 5), (5, 2), (6, None), (7, None)):
+        args = list(good)
+        args[k] = bad
+        assert f(*args) == _lib.ERR_ARGUMENT, (k, bad)
+    assert lib.psipm_set_factor_tc(None, 3) == _lib.ERR_ARGUMENT
 
 
 def test_static_matvec_rejects_null_and_oversized_arguments(lib):
