@@ -288,6 +288,11 @@ void syrk_update_tc(float* F, int r, int k0, int kb, int jend, int passes, int* 
                                         (int)kTcSmem));
         PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_tc<1, kStages1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kTcSmem));
+        // the largest shared-memory carveout: three 65 KB CTAs per SM
+        PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_tc<3, kStages3>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
+        PSIPM_CUDA(cudaFuncSetAttribute(k_syrk_tc<1, kStages1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
         attributes_set = true;
     }
     const int base = k0 + kb;
