@@ -22,6 +22,11 @@ Keys of the JSON line:
              (psipm_b200.learned, trained on solver traces of other seeds of
              this LP family) over --selector-steps solves; `value` stays the
              plain spectral rule;
+* learned_fp32  the metric's other arm: the learned selector with the FP32
+             preconditioner (FP64 PCG around an FP32 factor whose large
+             fronts' updates run on the tensor cores, FP32 sweeps) over
+             --fp32-steps solves, each bounded by --fp32-time-limit seconds
+             (a solve that hits it reports status "time-limit");
 * cpu_baseline  the CPU oracle (reference algorithm, SuperLU stand-in
              factor) timed on a bounded sample of the same LP (its first K
              outer iterations), next to the device's time for the same K
@@ -86,6 +91,10 @@ def parse():
                          "'none': no learned arm)")
     ap.add_argument("--selector-window", type=float, default=None)
     ap.add_argument("--selector-steps", type=int, default=3)
+    ap.add_argument("--fp32-steps", type=int, default=1,
+                    help="solves of the FP32 arm (learned selector + FP32 factor on the tensor cores)")
+    ap.add_argument("--fp32-time-limit", type=float, default=60.0,
+                    help="seconds per FP32-arm solve before it is reported as a time limit")
     return ap.parse_args()
 
 
@@ -324,6 +333,35 @@ def run_ours(args, rank, world, local_rank):
                    "window": window, "pcg_iterations_per_step": lpcg / k, "learned_refreshes_per_step": lref / k,
                    "fallbacks_per_step": lfb / k, "objective": sol_l.obj, "status": sol_l.status,
                    "speedup_vs_plain": per_step / max_over_ranks(lt / k)}
+    # ---- learned selector + FP32 factor and sweeps (the metric's other arm) ----
+    fp32 = None
+    if args.fp32_steps > 0:
+        from psipm_b200 import _lib
+
+        dev32 = NormalEquationsDevice(lp.A, device=local_rank, precision=_lib.FP32_PRECOND)
+        ft, fpcg, fstatus, fobj = 0.0, 0, [], None
+        try:
+            for _ in range(args.fp32_steps):
+                torch.cuda.synchronize()
+                dev32.timer_start()
+                solver32 = GpuSpectralStableColumnPreconditioner(lp.A, protected=~lp.pos, dev=dev32,
+                                                                 precision=_lib.FP32_PRECOND, selector=model,
+                                                                 selector_window=window)
+                sol32 = psipm_solve_resident(lp, solver32, tol=args.tol, time_limit=args.fp32_time_limit)
+                ft += dev32.timer_stop()
+                fpcg += solver32.pcg_total_iterations
+                fstatus.append(sol32.status)
+                fobj = sol32.obj
+                flush_l2()
+        finally:
+            dev32.close()
+        k = args.fp32_steps
+        fp32 = {"value": max_over_ranks(ft / k), "unit": "s", "steps": k,
+                "precision": "FP32_PRECOND (FP64 PCG, FP32 factor with 3xTF32 tensor-core updates, FP32 sweeps)",
+                "selector": os.path.basename(model.path) if model is not None else None,
+                "status": fstatus, "objective": fobj, "pcg_iterations_per_step": fpcg / k,
+                "time_limit_s": args.fp32_time_limit,
+                "speedup_vs_plain_fp64": per_step / max_over_ranks(ft / k)}
     # ---- end to end through the public API, host buffers ----------------------
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -379,6 +417,7 @@ def run_ours(args, rank, world, local_rank):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "learned_selector": learned,
+            "learned_fp32": fp32,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "lp_per_s": world / per_step,

@@ -755,9 +755,9 @@ void analyse(psipm_handle* h) {
     // handle's precision)
     h->pval.reserve(std::max<int64_t>(1, s.nentries));
     auto reserve_factor = [&](auto& fs) {
-        fs.ms.reserve(std::max<int64_t>(1, s.nentries));
-        fs.G.reserve(std::max<int64_t>(1, s.panel_total));
-        fs.GT.reserve(std::max<int64_t>(1, s.panel_total));
+        fs.ms.fit(std::max<int64_t>(1, s.nentries));
+        fs.G.fit(std::max<int64_t>(1, s.panel_total));
+        fs.GT.fit(std::max<int64_t>(1, s.panel_total));
         fs.xp.reserve(h->m);
         fs.yp.reserve(h->m);
         fs.dscp.reserve(h->m);
@@ -832,7 +832,7 @@ void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
         LAUNCH(h, k_front_extend_add<T><<<std::min(blocks_for(n2, 256), 8192), 256, 0, st>>>(
                       F, r, fa.update + s.update_off[ch], rc, fa.relind + s.uvec_off[ch]));
     }
-    const size_t trsm_smem = 2 * kNB * (kNB + 1) * sizeof(T);
+    const size_t trsm_smem = kNB * (kNB + 1) * sizeof(T);
     const size_t syrk_smem = 2 * kNB * (kNB + 1) * sizeof(T);
     // Cholesky of the diagonal block at k0 and the rows below it
     auto panel_step = [&](int k0, int kb) {
@@ -880,7 +880,7 @@ void factor_big_front(psipm_handle* h, int sn, const FactorArgs<T>& fa) {
     T* G = fa.G + s.panel_off[sn];
     const int nblk = (c + kGB - 1) / kGB;
     const size_t g_smem = 2 * kGB * (kGB + 1) * sizeof(T);
-    LAUNCH(h, k_diag_block_inv<T><<<nblk, 256, g_smem + 4 * kGB * sizeof(T), st>>>(F, r, c, fa.dinv));
+    LAUNCH(h, k_diag_block_inv<T><<<nblk, kGB, kGB * (kGB + 1) * sizeof(T), st>>>(F, r, c, fa.dinv));
     LAUNCH(h, k_g_init<T><<<dim3((c + 31) / 32, (r + 31) / 32), dim3(32, 8), 0, st>>>(F, r, c, fa.dinv, G));
     if (r > c)
         LAUNCH(h, k_g_convert<T><<<blocks_for(r - c, kGB), 256, g_smem, st>>>(r, c, fa.dinv, nblk - 1, G));
@@ -902,8 +902,8 @@ int factor_numeric(psipm_handle* h, double delta, int start_shift) {
     FactorStore<T>& fs = fstore(h, tag);
     // multifrontal workspace: update matrices, one level's fronts, the
     // diagonal-block inverses of a big front
-    fs.update.reserve(std::max<int64_t>(1, s.update_total));
-    fs.front.reserve(std::max<int64_t>(1, h->front_total));
+    fs.update.fit(std::max<int64_t>(1, s.update_total));
+    fs.front.fit(std::max<int64_t>(1, h->front_total));
     fs.dinv.reserve((int64_t)(s.max_cols / kGB + 1) * kGB * kGB);
     if (s.nentries)
         LAUNCH(h, k_assemble_entries<<<blocks_for(s.nentries, 256), 256, 0, st>>>(
@@ -1519,13 +1519,35 @@ int psipm_factor(psipm_handle* h, double delta, int32_t start_shift, int32_t* sh
         require(h->have_theta, PSIPM_ERR_STATE, "factor before set_theta");
         require(!h->tree_mode, PSIPM_ERR_STATE, "the handle uses the tree preconditioner (psipm_tree_factor)");
         h->have_factor = false;  // until this factorisation succeeds (a failed one leaves no factor)
-        if (h->core_dirty || !h->have_symbolic) analyse(h);
-        h->delta = delta;
+        int used = -1;
         Symbolic& s = h->sym;
         cudaStream_t st = h->stream;
-        PSIPM_CUDA(cudaEventRecord(h->ev0, st));
-        int used = h->precision != PSIPM_FP64 ? factor_numeric<float>(h, delta, start_shift)
-                                                      : factor_numeric<double>(h, delta, start_shift);
+        try {
+            if (h->core_dirty || !h->have_symbolic) analyse(h);
+            h->delta = delta;
+            PSIPM_CUDA(cudaEventRecord(h->ev0, st));
+            used = h->precision != PSIPM_FP64 ? factor_numeric<float>(h, delta, start_shift)
+                                              : factor_numeric<double>(h, delta, start_shift);
+        } catch (const Failure& f) {
+            if (f.code == PSIPM_ERR_MEMORY) {
+                // give every factor buffer back, so that a smaller core fits
+                // next time; the next factorisation analyses afresh
+                (void)cudaStreamSynchronize(st);
+                auto drop = [](auto& fs) {
+                    fs.ms.release();
+                    fs.G.release();
+                    fs.GT.release();
+                    fs.update.release();
+                    fs.front.release();
+                    fs.fvec.release();
+                    fs.dinv.release();
+                };
+                drop(h->f64);
+                drop(h->f32);
+                h->have_symbolic = false;
+            }
+            throw;
+        }
         PSIPM_CUDA(cudaEventRecord(h->ev1, st));
         PSIPM_CUDA(cudaEventSynchronize(h->ev1));
         float ms = 0.f;

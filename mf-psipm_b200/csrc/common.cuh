@@ -57,6 +57,13 @@ struct DevBuf {
         }
         n = count;
     }
+    // As reserve, but a buffer more than twice the size asked for (and above
+    // 64 MB) is given back first: a smaller factor after a larger one does
+    // not keep the larger one's memory.
+    void fit(size_t count) {
+        if (p && n > 2 * count && n * sizeof(T) > (size_t(64) << 20)) release();
+        reserve(count);
+    }
     void upload(const T* host, size_t count, cudaStream_t s) {
         reserve(count);
         if (count) PSIPM_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));

@@ -241,71 +241,88 @@ __global__ void k_front_extend_add(T* __restrict__ F, int r, const T* __restrict
     }
 }
 
-// Cholesky of the diagonal block F[k0:k0+kb, k0:k0+kb] in shared memory (1 CTA)
+// Cholesky of the diagonal block F[k0:k0+kb, k0:k0+kb] in shared memory (1 CTA).
+// Right-looking with the columns left unscaled until the end, so each step
+// is one update and one barrier: step k subtracts D[i][k] D[j][k] / d_k from
+// the trailing triangle (d_k = D[k][k], final after step k - 1; every thread
+// reads it and takes the same branch), then L[i][k] = D[i][k] / sqrt(d_k).
+// A non-positive or non-finite pivot sets `fail` and is replaced by 1.
 template <typename T>
 __global__ void __launch_bounds__(256) k_potrf_diag(T* __restrict__ F, int r, int k0, int kb, int* fail) {
     __shared__ T D[kNB][kNB + 1];
-    __shared__ int bad;
+    __shared__ T piv[kNB];
     const int tid = threadIdx.x;
-    if (tid == 0) bad = 0;
     for (int q = tid; q < kb * kb; q += blockDim.x) {
         const int i = q % kb, j = q / kb;
         D[i][j] = i >= j ? F[(long long)(k0 + j) * r + (k0 + i)] : (T)0;
     }
     __syncthreads();
+    bool bad = false;
     for (int k = 0; k < kb; ++k) {
-        if (tid == 0) {
-            T d = D[k][k];
-            if (!(d > (T)0) || !isfinite((double)d)) {
-                bad = 1;
-                d = (T)1;
-            }
-            D[k][k] = sqrt(d);
+        T d = D[k][k];
+        if (!(d > (T)0) || !isfinite((double)d)) {
+            bad = true;
+            d = (T)1;
         }
-        __syncthreads();
-        const T inv = (T)1 / D[k][k];
-        for (int i = k + 1 + tid; i < kb; i += blockDim.x) D[i][k] *= inv;
-        __syncthreads();
+        if (tid == 0) piv[k] = d;
+        const T invd = (T)1 / d;
         const int rem = kb - k - 1;
         for (int q = tid; q < rem * rem; q += blockDim.x) {
             const int i = k + 1 + q % rem, j = k + 1 + q / rem;
-            if (i >= j) D[i][j] -= D[i][k] * D[j][k];
+            if (i >= j) D[i][j] -= D[i][k] * invd * D[j][k];
         }
         __syncthreads();
     }
     for (int q = tid; q < kb * kb; q += blockDim.x) {
         const int i = q % kb, j = q / kb;
-        if (i >= j) F[(long long)(k0 + j) * r + (k0 + i)] = D[i][j];
+        if (i >= j) {
+            const T sj = sqrt(piv[j]);
+            F[(long long)(k0 + j) * r + (k0 + i)] = i == j ? sj : D[i][j] / sj;
+        }
     }
     if (tid == 0 && bad) atomicOr(fail, 1);
 }
 
 // panel: F[i, k0:k0+kb] <- F[i, k0:k0+kb] L_kk^{-T} for rows i >= k0+kb
-// (one thread per row, 64 rows per CTA; dynamic shared memory 2 x 64 x 65 T)
+// (one thread per row, 64 rows per CTA; dynamic shared memory 64 x 65 T).
+// Each thread keeps its row in registers and eliminates column by column
+// (x_j = b_j / L_jj, then b_l -= x_j L_lj for every l > j): 64 dependent
+// steps whose 63, 62, ... updates are independent.  Past kb the block is the
+// identity, so the fully unrolled loop serves every kb <= 64.
 constexpr int kTrsmRows = 64;
 template <typename T>
 __global__ void __launch_bounds__(kTrsmRows) k_trsm_panel(T* __restrict__ F, int r, int k0, int kb) {
     extern __shared__ __align__(16) unsigned char smem_f[];
-    T* Lk = reinterpret_cast<T*>(smem_f);  // [64][65]
-    T* X = Lk + kNB * (kNB + 1);           // [64][65]
+    T* Lk = reinterpret_cast<T*>(smem_f);  // Lk[l * 65 + j] = L[l][j]
+    __shared__ T rdiag[kNB];
     const int tid = threadIdx.x;
     const int row0 = k0 + kb + blockIdx.x * kTrsmRows;
-    for (int q = tid; q < kb * kb; q += blockDim.x) {
-        const int i = q % kb, j = q / kb;
-        Lk[i * (kNB + 1) + j] = F[(long long)(k0 + j) * r + (k0 + i)];
+    for (int q = tid; q < kNB * kNB; q += blockDim.x) {
+        const int l = q % kNB, j = q / kNB;
+        T v;
+        if (l < kb && j < kb)
+            v = l >= j ? F[(long long)(k0 + j) * r + (k0 + l)] : (T)0;
+        else
+            v = l == j ? (T)1 : (T)0;
+        Lk[l * (kNB + 1) + j] = v;
     }
     const int i = row0 + tid;
-    for (int j = 0; j < kb; ++j) X[tid * (kNB + 1) + j] = i < r ? F[(long long)(k0 + j) * r + i] : (T)0;
+    T x[kNB];
+#pragma unroll
+    for (int j = 0; j < kNB; ++j) x[j] = (i < r && j < kb) ? F[(long long)(k0 + j) * r + i] : (T)0;
     __syncthreads();
+    if (tid < kNB) rdiag[tid] = (T)1 / Lk[tid * (kNB + 1) + tid];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kNB; ++j) {
+        x[j] *= rdiag[j];
+#pragma unroll
+        for (int l = j + 1; l < kNB; ++l) x[l] -= x[j] * Lk[l * (kNB + 1) + j];
+    }
     if (i < r) {
-        T* x = X + tid * (kNB + 1);
-        for (int j = 0; j < kb; ++j) {
-            T s = x[j];
-            const T* lj = Lk + j * (kNB + 1);
-            for (int l = 0; l < j; ++l) s -= x[l] * lj[l];
-            x[j] = s / lj[j];
-        }
-        for (int j = 0; j < kb; ++j) F[(long long)(k0 + j) * r + i] = x[j];
+#pragma unroll
+        for (int j = 0; j < kNB; ++j)
+            if (j < kb) F[(long long)(k0 + j) * r + i] = x[j];
     }
 }
 
@@ -386,35 +403,36 @@ __global__ void k_extract_update(const T* __restrict__ F, int r, int c, T* __res
 // of X above the diagonal block of J are zero, so step J touches rows >= 64 J.
 constexpr int kGB = 64;
 
-// D_J^T for every diagonal block J (row n holds column n of D_J), zero past c.
-// One CTA per block; thread (p, j) computes column j, the k-sums split in four.
+// D_J^T for every diagonal block J (row n holds column n of D_J).
+// One CTA of kGB threads per block; past c the block is the identity.
 template <typename T>
-__global__ void __launch_bounds__(256) k_diag_block_inv(const T* __restrict__ F, int r, int c, T* __restrict__ DT) {
-    extern __shared__ __align__(16) unsigned char smem_d[];  // 2 * kGB * (kGB + 1) + 4 * kGB scalars
+__global__ void __launch_bounds__(kGB) k_diag_block_inv(const T* __restrict__ F, int r, int c, T* __restrict__ DT) {
+    extern __shared__ __align__(16) unsigned char smem_d[];  // kGB * (kGB + 1) scalars
     T(*L)[kGB + 1] = reinterpret_cast<T(*)[kGB + 1]>(smem_d);
-    T(*X)[kGB + 1] = L + kGB;
-    T(*part)[kGB] = reinterpret_cast<T(*)[kGB]>(X + kGB);
+    __shared__ T rdiag[kGB];
     const int jc0 = blockIdx.x * kGB, jn = min(kGB, c - jc0);
     const int tid = threadIdx.x;
     for (int q = tid; q < kGB * kGB; q += blockDim.x) {
         const int i = q % kGB, j = q / kGB;
         L[i][j] = (i < jn && j < jn) ? (i >= j ? F[(long long)(jc0 + j) * r + jc0 + i] : (T)0) : (T)(i == j);
-        X[i][j] = 0;
     }
     __syncthreads();
-    const int j = tid % kGB, p = tid / kGB;
-    for (int i = 0; i < kGB; ++i) {
-        // X[i][j] = (delta_ij - sum_{k<i} L[i][k] X[k][j]) / L[i][i]; X[k][j] = 0 for k < j
-        T acc = 0;
-        for (int k = p; k < i; k += 4) acc += L[i][k] * X[k][j];
-        part[p][j] = acc;
-        __syncthreads();
-        if (p == 0 && i >= j)
-            X[i][j] = ((T)(i == j) - ((part[0][j] + part[1][j]) + (part[2][j] + part[3][j]))) / L[i][i];
-        __syncthreads();
+    rdiag[tid] = (T)1 / L[tid][tid];
+    __syncthreads();
+    // thread n: column n of D = L^{-1} by forward elimination of e_n in
+    // registers (x_k = x_k / L_kk, then x_i -= L_ik x_k for i > k)
+    T x[kGB];
+#pragma unroll
+    for (int k = 0; k < kGB; ++k) x[k] = (T)(k == tid);
+#pragma unroll
+    for (int k = 0; k < kGB; ++k) {
+        x[k] *= rdiag[k];
+#pragma unroll
+        for (int i = k + 1; i < kGB; ++i) x[i] -= L[i][k] * x[k];
     }
-    T* out = DT + (long long)blockIdx.x * kGB * kGB;
-    for (int q = tid; q < kGB * kGB; q += blockDim.x) out[q] = X[q % kGB][q / kGB];  // out[n][k] = D[k][n]
+    T* out = DT + (long long)blockIdx.x * kGB * kGB + (long long)tid * kGB;  // out[n][k] = D[k][n]
+#pragma unroll
+    for (int k = 0; k < kGB; ++k) out[k] = x[k];
 }
 
 // B into G: rows < c hold D_J on their diagonal block and zeros elsewhere,
