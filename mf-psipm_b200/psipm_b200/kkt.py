@@ -249,6 +249,7 @@ class GpuStableActiveColumnPreconditioner:
         self.core_history = []
         self.tie_straddles = 0
         self.memory_caps = 0  # core targets lowered because a factor did not fit in device memory
+        self._largest_fit = 0  # size of the largest core factored so far
         # learned selector (no counterpart in the reference): a SelectorModel that
         # re-scores the candidates before the rule's refresh; a learned core that
         # turns out poor by the rule's own signals suspends it for
@@ -367,6 +368,8 @@ class GpuStableActiveColumnPreconditioner:
                 # the factor of this core does not fit in device memory: cap the
                 # core below its size and refresh at the next factorisation
                 cap = max(int(self.mandatory.size), int(0.8 * self.core.size))
+                if self._largest_fit < self.core.size:  # never below a core whose factor fitted
+                    cap = max(cap, self._largest_fit)
                 self.max_core_target = min(self.max_core_target, cap)
                 self.core_target = min(self.core_target, cap)
                 self._initialized = False
@@ -379,6 +382,7 @@ class GpuStableActiveColumnPreconditioner:
                 raise KKTSolveError(f"Cholesky failed even with a 1e-2 shift ({exc})") from exc
             raise KKTSolveError(str(exc)) from exc
         self.stats["not_pd"] += used - start
+        self._largest_fit = max(self._largest_fit, int(self.core.size))
         self._shift = SHIFTS[used]
         if used > 0:
             self.n_shifted += 1

@@ -123,3 +123,22 @@ def test_invalid_options_raise_like_the_reference(lp):
         GpuSpectralStableColumnPreconditioner(lp.A, dev=FakeDevice(lp.A), cg_tol=0.5, cg_tol_max=0.1)
     with pytest.raises(ValueError):
         GpuSpectralStableColumnPreconditioner(lp.A, protected=np.ones(3, bool), dev=FakeDevice(lp.A))
+
+
+def test_memory_cap_keeps_the_largest_core_that_fitted(lp):
+    """A factor that does not fit lowers the core target to 0.8 of that core,
+    but never below the largest core factored so far."""
+    dev = FakeDevice(lp.A)
+    solver = make(lp, dev)
+    m = lp.A.shape[0]
+    theta = np.ones(lp.A.shape[1])
+    solver.factorize(theta, 1.0)
+    fitted = solver.core.size
+    assert fitted > 0
+    solver.core = np.arange(int(1.1 * fitted) + 5, dtype=np.int64)  # a larger core
+    dev.fail["factor"] = [_lib.ERR_MEMORY]
+    with pytest.raises(KKTSolveError):
+        solver._factor_current(theta, 1.0)
+    assert solver.memory_caps == 1
+    assert solver.core_target >= fitted and solver.max_core_target >= fitted
+    assert solver.core_target <= int(1.1 * fitted) + 5
