@@ -18,6 +18,9 @@ Keys of the JSON line:
 * roofline   the persistent PCG kernel (k_pcg): algorithmic bytes of all
              its launches / its CUDA-event time, against the measured HBM
              copy bandwidth;
+* spmv       the operator pair H p = A (w o (A' p)) + delta p inside k_pcg:
+             its algorithmic bytes per product / its time per product (the
+             kernel's own clock marks), against the same bandwidth;
 * learned_selector  the same solve with the learned active-column selector
              (psipm_b200.learned, trained on solver traces of other seeds of
              this LP family) over --selector-steps solves; `value` stays the
@@ -62,12 +65,12 @@ WORKLOAD = ("min-cost flow LP, 200x250 directed grid (both orientations) + 10% r
             "preconditioner, FP64")
 HBM_FALLBACK = 6650.0
 # DRAM traffic of k_pcg, from one ncu capture on a B200 of the 151st k_pcg launch
-# of `python bench.py --steps 1 --warmup 0 --no-cpu-baseline`:
+# of `python bench.py --steps 1 --warmup 0 --no-cpu-baseline --selector none --fp32-steps 0`:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:k_pcg -s 150 -c 1 ...
-# read 66,833,828,096 B + written 767,213,824 B in 50.275744 ms.  The bench scales
+# read 14,438,526,720 B + written 167,321,344 B in 10.243744 ms.  The bench scales
 # this rate by its own average launch duration to give bytes per launch.
-KPCG_DRAM_BYTES_PER_S = (66_833_828_096 + 767_213_824) / 0.050275744
+KPCG_DRAM_BYTES_PER_S = (14_438_526_720 + 167_321_344) / 0.010243744
 
 
 def parse():
@@ -297,7 +300,7 @@ def run_ours(args, rank, world, local_rank):
     launches0 = dev.kernel_launches
     total = 0.0
     sols = []
-    pcg_s = pcg_b = 0.0
+    pcg_s = pcg_b = hp_s = 0.0
     pcg_launches = pcg_its = 0
     for _ in range(args.steps):
         torch.cuda.synchronize()
@@ -309,6 +312,7 @@ def run_ours(args, rank, world, local_rank):
         pcg_b += solver.pcg_bytes
         pcg_launches += solver.pcg_launches
         pcg_its += solver.pcg_total_iterations
+        hp_s += float(solver.pcg_phase_seconds[0])
         flush_l2()
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -386,6 +390,18 @@ def run_ours(args, rank, world, local_rank):
             "note": "the operator (~10 MB) is L2-resident and the factor panels (0.6-1 GB read per "
                     "preconditioner application) stream from HBM; the supernodal sweeps below the two "
                     "top tree levels are latency bound, so the HBM fraction stays low"}
+    from psipm_b200.roofline import hp_bytes
+
+    b_hp = hp_bytes(m, n, lp.A.nnz)
+    hp_gbs = b_hp * pcg_its / hp_s / 1e9 if hp_s > 0 else None
+    spmv = {"bound": "hbm", "achieved": hp_gbs, "peak": peak, "unit": "GB/s",
+            "frac": (hp_gbs / peak) if hp_gbs else None, "bytes_per_product": b_hp,
+            "us_per_product": 1e6 * hp_s / pcg_its if pcg_its else None,
+            "kernel": "k_pcg operator phases: H p = A (w o (A' p)) + delta p with its dot-product reduction",
+            "timing": "the PCG kernel's own %globaltimer marks (block 0) around each iteration's operator "
+                      "pass, summed over the timed solves",
+            "note": "this LP's operator (A twice, w, t, p, q: ~20 MB) stays in L2, so the HBM figure is a "
+                    "byte rate, not DRAM traffic"}
     line = None
     if rank == 0:
         sol0 = sols[-1]
@@ -414,6 +430,7 @@ def run_ours(args, rank, world, local_rank):
                        "objective": sol0.obj, "status": sol0.status,
                        "pcg_iterations_per_step": pcg_its / args.steps},
             "roofline": roof,
+            "spmv": spmv,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "learned_selector": learned,
