@@ -6,8 +6,9 @@
 
 namespace psipm {
 
-// Status bits a tensor-core kernel raises in *err (the factor's fail word is
-// not touched): a wait on the tensor core's completion barrier ran out.
+// Status bit a tensor-core kernel ORs into *err when a wait on the tensor
+// core's completion barrier ran out.  The factor passes its fail word, whose
+// bit 0 marks a failed pivot; the host tells the two apart.
 constexpr int kTcErrWait = 1 << 20;
 
 // F[i, j] -= sum_{k < kb} F[i, k0 + k] F[j, k0 + k] for k0 + kb <= j <= i < r,
