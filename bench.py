@@ -84,7 +84,9 @@ def parse():
                     help="grid: the 200x250 network LP (the default line); batch: uneven random LPs "
                          "served several at a time, against the same LPs one after another")
     ap.add_argument("--count", type=int, default=256, help="LPs of the batch workload")
-    ap.add_argument("--workers", type=int, default=8, help="LPs in flight in the batch workload")
+    ap.add_argument("--workers", type=int, default=8,
+                    help="LPs in flight in the batch workload (0: choose the schedule with psipm_b200.batch.autotune "
+                         "on 16 LPs of the batch, outside the timed region)")
     ap.add_argument("--rows", type=int, default=200)
     ap.add_argument("--cols", type=int, default=250)
     ap.add_argument("--cpu-sample-outer", type=int, default=2)
@@ -449,14 +451,19 @@ def run_batch(args, rank, world, local_rank):
     import torch
 
     from psipm_b200 import synthetic
-    from psipm_b200.batch import solve_batch, solve_sequential
+    from psipm_b200.batch import autotune, solve_batch, solve_sequential
     from psipm_b200.replicas import max_over_ranks, partition_by_nnz
 
     torch.cuda.set_device(local_rank)
     lps = synthetic.random_lp_batch(count=args.count, seed=4000)
     mine = [lps[k] for k in partition_by_nnz([lp.A.nnz for lp in lps], world)[rank]]
-    solve_batch(mine[: min(len(mine), args.workers)], workers=args.workers, device=local_rank)  # warm-up
-    bat = solve_batch(mine, workers=args.workers, device=local_rank)
+    workers, grid_blocks, tuned = args.workers, None, None
+    if workers <= 0:  # the tuner's trials also warm the device up
+        tuned = autotune(mine, sample=16, device=local_rank)
+        workers, grid_blocks = tuned.workers, tuned.grid_blocks
+    else:
+        solve_batch(mine[: min(len(mine), workers)], workers=workers, device=local_rank)  # warm-up
+    bat = solve_batch(mine, workers=workers, device=local_rank, grid_blocks=grid_blocks)
     seconds = max_over_ranks(bat.seconds)
     seq = solve_sequential(mine, device=local_rank) if world == 1 else None
     if rank != 0:
@@ -466,7 +473,10 @@ def run_batch(args, rank, world, local_rank):
         "unit": "LP/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * seconds,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{len(lps)} uneven random LPs, m ~ U{{500..5000}}, n = 3m, 5 nonzeros per column, "
-                               f"seeds 4001..{4000 + len(lps)}", "workers": args.workers, "tol": 1e-8},
+                               f"seeds 4001..{4000 + len(lps)}", "workers": workers, "grid_blocks": grid_blocks,
+                   "tol": 1e-8},
+        "autotune": None if tuned is None else {"workers": tuned.workers, "grid_blocks": tuned.grid_blocks,
+                                                 "trials": tuned.trials},
         "p50_s": bat.percentile(50), "p99_s": bat.percentile(99),
         "optimal": sum(s == "optimal" for s in bat.status), "errors": bat.errors[:5],
         "sequential": None if seq is None else {"value": seq.lps_per_second, "p50_s": seq.percentile(50),

@@ -12,7 +12,9 @@ one LP's launches idling the rest of the GPU.
 
 :func:`solve_batch` returns per-LP wall times (submission to result) and the
 aggregate LPs per second; :func:`solve_sequential` is the baseline, one LP
-at a time with the whole GPU.
+at a time with the whole GPU.  :func:`autotune` picks the schedule (LPs in
+flight and each LP's share of the persistent grid) by timing candidates on a
+sample of the batch.
 """
 
 from __future__ import annotations
@@ -107,3 +109,59 @@ def solve_batch(lps, workers: int = 8, tol: float = 1e-8, device: int = 0,
 def solve_sequential(lps, tol: float = 1e-8, device: int = 0) -> BatchResult:
     """The baseline: one LP at a time, each with the whole GPU."""
     return solve_batch(lps, workers=1, tol=tol, device=device, grid_blocks=0)
+
+
+@dataclass
+class Schedule:
+    workers: int        # LPs in flight
+    grid_blocks: int    # persistent-kernel blocks per LP (psipm_set_grid; 0 = the whole co-resident grid)
+    lps_per_second: float
+    trials: List[dict] = field(default_factory=list)
+
+
+def schedule_candidates(sms: int, max_workers: int = 16) -> List[tuple]:
+    """(workers, grid_blocks) pairs the tuner times: 1, 2, 4, ... LPs in flight,
+    each with its share of the co-resident grid (4 blocks per SM divided among
+    them) and with half that share."""
+    out = []
+    w = 1
+    while w <= max_workers:
+        share = max(8, (4 * sms) // w)
+        out.append((w, 0 if w == 1 else share))
+        if w > 1 and share // 2 >= 8:
+            out.append((w, share // 2))
+        w *= 2
+    return out
+
+
+def autotune(lps, sample: int = 16, candidates: Optional[List[tuple]] = None, tol: float = 1e-8,
+             device: int = 0, run=None) -> Schedule:
+    """Choose the batch schedule by timing each candidate on the same sample.
+
+    The sample is ``sample`` LPs spread over the batch (every k-th, so their
+    sizes follow the batch's distribution); each candidate solves the whole
+    sample with :func:`solve_batch`, and the schedule with the most LPs per
+    second wins (ties: fewer workers).  ``run(lps, workers, grid_blocks)``
+    replaces :func:`solve_batch` (tests use a timing model).
+    """
+    if not lps:
+        raise ValueError("no LPs to tune on")
+    if candidates is None:
+        import torch
+
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+        candidates = schedule_candidates(sms)
+    if run is None:
+        def run(sub, workers, grid_blocks):
+            return solve_batch(sub, workers=workers, tol=tol, device=device, grid_blocks=grid_blocks)
+    step = max(1, len(lps) // max(1, sample))
+    sub = list(lps[::step])[:max(1, sample)]
+    best, trials = None, []
+    for workers, grid_blocks in candidates:
+        res = run(sub, workers, grid_blocks)
+        rate = res.lps_per_second
+        trials.append(dict(workers=workers, grid_blocks=grid_blocks, lps_per_second=rate,
+                           optimal=sum(st == "optimal" for st in res.status)))
+        if best is None or rate > best[2] * (1.0 + 1e-9):
+            best = (workers, grid_blocks, rate)
+    return Schedule(best[0], best[1], best[2], trials)
