@@ -5,8 +5,11 @@ The reference's column-generation drivers (``retrospective_solve`` and
 restricted master LPs on a working set of columns with ``psipm_solve`` and
 price the remaining columns with the duals after each converged master.
 This module is the device counterpart of that loop in its basic form (no
-retrospective elimination, no warm start mapping):
+retrospective elimination, no warm start mapping between masters):
 
+* the first working set is the covering crash support when asked for and
+  the LP is a covering LP (:func:`covering_crash`), else the free columns and
+  the cheapest others;
 * the master is the LP restricted to the working columns plus one
   artificial column ``+e_i`` and one ``-e_i`` per row at a large cost, so
   every master is feasible (the reference's ``cg_artificial_cost``);
@@ -48,6 +51,96 @@ class ColumnGenerationResult:
     history: List[dict] = field(default_factory=list)
 
 
+_EPS = float(np.finfo(float).eps)
+_POS_FLOOR = 8.0 * _EPS
+
+
+def covering_crash(lp) -> Optional[np.ndarray]:
+    """A feasible starting support for a covering LP, or None.
+
+    The reference's crash (``_covering_crash_mask``, psipm_active_pool.py:
+    3436-3533) applies to an LP whose rows have positive demand b_i, whose
+    structural columns are nonnegative and whose every row has a zero-cost,
+    unbounded, negative singleton surplus column.  An unbounded structural
+    column of nonnegative cost never needs to exceed max_i b_i / a_ij over its
+    rows, so that value caps it; each row then takes the structural column
+    that can cover it alone at its cap with the least cap cost per unit of
+    covered demand (the first such column in index order on ties), and the
+    surplus columns absorb the overcoverage.  The selected columns plus all
+    surplus columns are a feasible restricted master.  This is the same
+    decision rule, computed over the CSR arrays at once instead of row by row.
+    """
+    A = lp.A.tocsc(copy=True)
+    A.eliminate_zeros()
+    m, n = A.shape
+    b, c, u = np.asarray(lp.b, float), np.asarray(lp.c, float), np.asarray(lp.u, float)
+    if m == 0 or np.any(b <= 0.0) or not np.all(lp.pos):
+        return None
+    nnz_col = np.diff(A.indptr)
+    scale = 1.0 + float(np.abs(c).max(initial=0.0))
+    single = np.flatnonzero((nnz_col == 1) & (np.abs(c) <= 100.0 * _EPS * scale) & ~np.isfinite(u))
+    srow = A.indices[A.indptr[single]]
+    sval = A.data[A.indptr[single]]
+    neg = sval < 0.0
+    single, srow, sval = single[neg], srow[neg], sval[neg]
+    # per row the surplus of largest |value|, the lowest column index among equals
+    order = np.lexsort((single, sval, srow))  # by row, then most negative value, then index
+    first = np.ones(order.size, dtype=bool)
+    first[1:] = srow[order][1:] != srow[order][:-1]
+    pick = order[first]
+    surplus = np.full(m, -1, dtype=np.int64)
+    surplus_value = np.zeros(m)
+    surplus[srow[pick]] = single[pick]
+    surplus_value[srow[pick]] = sval[pick]
+    if np.any(surplus < 0):
+        return None
+    structural = np.ones(n, dtype=bool)
+    structural[surplus] = False
+    cols = np.repeat(np.arange(n), nnz_col)
+    if np.any((A.data < -100.0 * _EPS) & structural[cols]):
+        return None
+    cap = u.copy()
+    ratio_max = np.full(n, np.inf)
+    nonempty = nnz_col > 0
+    if nonempty.any():
+        ratio_max[nonempty] = np.maximum.reduceat(b[A.indices] / A.data, A.indptr[:-1][nonempty])
+    implied = structural & ~np.isfinite(cap) & (c >= -100.0 * _EPS * scale)
+    cap[implied] = ratio_max[implied]
+    usable_col = structural & np.isfinite(cap) & (cap > 0.0)
+    R = A.tocsr()
+    rows = np.repeat(np.arange(m), np.diff(R.indptr))
+    jj, aa = R.indices, R.data
+    tol = 100.0 * _EPS * (1.0 + np.abs(b))
+    ok = usable_col[jj] & (aa > 0.0)
+    contribution = np.where(ok, aa * np.where(ok, cap[jj], 0.0), 0.0)
+    ok &= contribution + tol[rows] >= b[rows]
+    if not np.all(np.bincount(rows[ok], minlength=m) > 0):
+        return None
+    score = np.full(jj.size, np.inf)
+    cj = np.where(ok, cap[jj], 0.0)
+    score[ok] = np.maximum(c[jj[ok]] * cj[ok], 0.0) / np.maximum(np.minimum(contribution[ok], b[rows[ok]]),
+                                                                   _POS_FLOOR)
+    # per row the first entry (CSR order) of least score among the valid ones
+    pos = np.arange(jj.size)
+    best_order = np.lexsort((pos, score, rows))
+    head = np.ones(best_order.size, dtype=bool)
+    head[1:] = rows[best_order][1:] != rows[best_order][:-1]
+    best = jj[best_order[head]]
+    selected = np.unique(best)
+    coverage = np.asarray(A[:, selected] @ cap[selected]).ravel()
+    over = coverage - b
+    if np.any(over < -tol):
+        return None
+    with np.errstate(divide="ignore", invalid="ignore"):
+        surplus_x = over / (-surplus_value)
+    if np.any(~np.isfinite(surplus_x)) or np.any(surplus_x < 0.0):
+        return None
+    working = np.zeros(n, dtype=bool)
+    working[selected] = True
+    working[surplus] = True
+    return working
+
+
 def initial_working(lp, count: int) -> np.ndarray:
     """Free columns (never priced out) and the `count` cheapest others."""
     n = lp.A.shape[1]
@@ -74,12 +167,17 @@ def _master(lp, cols: np.ndarray, big: float) -> StandardLP:
 def column_generation_solve(lp, tol: float = 1e-8, initial: Optional[int] = None,
                             pricing_batch: Optional[int] = None, pricing_tol: Optional[float] = None,
                             max_rounds: int = 30, artificial_cost: Optional[float] = None,
-                            device: int = 0, solver_options: Optional[dict] = None) -> ColumnGenerationResult:
+                            device: int = 0, solver_options: Optional[dict] = None,
+                            crash: bool = False) -> ColumnGenerationResult:
+    """``crash=True`` starts a covering LP from :func:`covering_crash`'s
+    feasible support (the reference's ``sparse_cover_crash``, on by default
+    there, psipm_active_pool.py:3746-3749), else from the cheapest columns."""
     from .ipm_device import solve_standard
 
     started = time.perf_counter()
     m, n = lp.A.shape
-    working = initial_working(lp, max(256, m) if initial is None else initial)
+    start = covering_crash(lp) if crash else None
+    working = start.copy() if start is not None else initial_working(lp, max(256, m) if initial is None else initial)
     batch = max(1000, min(n, max(1, m // 2))) if pricing_batch is None else int(pricing_batch)
     ptol = max(tol, 1e-9) if pricing_tol is None else float(pricing_tol)
     big = (1e3 * (1.0 + float(np.abs(lp.c).max(initial=0.0)))) if artificial_cost is None else float(artificial_cost)

@@ -154,6 +154,46 @@ def main():
         make_hsd(PS, synthetic)
     if args.only in (None, "hsd_newton_m1600"):
         make_hsd_newton(synthetic)
+    if args.only in (None, "crash_masks"):
+        make_crash(PS, synthetic)
+
+
+CRASH_CASES = {
+    "cover_a": ("set_cover", dict(m=300, n=6000, seed=2101)),
+    "cover_b": ("set_cover", dict(m=120, n=2000, kmin=1, kmax=4, seed=2102)),
+    "cover_c": ("set_cover", dict(m=500, n=20000, zipf=1.5, seed=2103)),
+    "random": ("random_lp", dict(m=100, n=300, seed=2104)),  # not a covering LP: no crash
+    "cover_unbounded": ("set_cover", dict(m=200, n=4000, seed=2105)),  # upper bounds dropped: implied caps
+}
+
+
+def crash_lp(synthetic, name, family, kwargs):
+    """The LP of a crash case (the test rebuilds it the same way)."""
+    lp = getattr(synthetic, family)(**kwargs)
+    if name.endswith("_unbounded"):
+        lp.u[:] = np.inf
+        lp.box[:] = False
+        lp.c[np.diff(lp.A.tocsc().indptr) > 1] *= 1.0 + np.arange(int((np.diff(lp.A.tocsc().indptr) > 1).sum())) % 3
+    return lp
+
+
+def make_crash(PS, synthetic):
+    """The reference's covering crash support (_covering_crash_mask,
+    psipm_active_pool.py:3436-3533) on a few covering LPs and one LP it must
+    decline; the LPs are rebuilt from the generator's arguments."""
+    out = {}
+    for name, (family, kwargs) in CRASH_CASES.items():
+        lp0 = crash_lp(synthetic, name, family, kwargs)
+        lp = PS.StandardLP(c=lp0.c, A=lp0.A, b=lp0.b, u=lp0.u, pos=lp0.pos, box=lp0.box)
+        mask = PS._covering_crash_mask(lp)
+        out[f"{name}_family"] = family
+        out[f"{name}_kwargs"] = repr(kwargs)
+        out[f"{name}_none"] = mask is None
+        out[f"{name}_mask"] = np.zeros(0, dtype=bool) if mask is None else np.asarray(mask, dtype=bool)
+        print(f"crash {name}: {'none' if mask is None else int(mask.sum())} of {lp.A.shape[1]} columns")
+    path = os.path.join(HERE, "crash_masks.npz")
+    np.savez_compressed(path, **out)
+    print(f"crash_masks -> {os.path.getsize(path) / 1e3:.1f} kB")
 
 
 def make_result(PS, SSP, synthetic, name, family, kwargs):
