@@ -1,20 +1,21 @@
 // Trailing updates of the FP32 factor's large fronts on the 5th-generation
 // tensor cores (tcgen05.mma kind::tf32, accumulators in tensor memory).
 //
-// One CTA of 256 threads computes one 128 x 128 tile of
+// One CTA of 256 threads computes one 128 x 128 tile of the blocked
+// right-looking Cholesky's SYRK step
 //     F[i, j] -= sum_k P[i, k] P[j, k],   P = F[:, k0 : k0 + kb]
-// (the blocked right-looking Cholesky's SYRK step, psipm_active_pool.py:
-// 839-897 factors the same matrix with CHOLMOD on the CPU).  K runs in
-// stages of 32 FP32 values, the width of one 128-byte swizzled shared-memory
-// row.  While the tensor core works on one stage the threads already hold the
-// next stage's values in registers.  The threads load the column-major panel with coalesced
-// 4-byte loads (consecutive threads, consecutive rows), split each value into
-// a TF32 head (round to nearest) and the FP32 remainder, and store both as
-// K-major tiles in the canonical 128-byte swizzle; one elected thread issues
-// hi*hi + hi*lo + lo*hi (3xTF32: the products carry ~22 significant bits,
-// FP32-level) or hi*hi alone, and commits to a shared-memory barrier.  The
-// epilogue reads the accumulator out of tensor memory (32x32b.x32 loads) and
-// subtracts it from the front's lower triangle with coalesced accesses.
+// (the reference factors the same matrix with CHOLMOD on the CPU,
+// psipm_active_pool.py:839-897).  K runs in stages of 32 FP32 values, the
+// width of one 128-byte swizzled shared-memory row; while the tensor core
+// works on one stage, the threads already hold the next stage's values in
+// registers.  The threads load the column-major panel with coalesced 4-byte
+// loads (consecutive threads, consecutive rows), split each value into a TF32
+// head (round to nearest) and its FP32 remainder, and store both as K-major
+// tiles in the canonical 128-byte swizzle; one thread issues hi*hi + hi*lo +
+// lo*hi (3xTF32: the products carry ~22 significant bits, FP32-level) or
+// hi*hi alone, and commits to a shared-memory barrier.  The epilogue reads
+// the accumulator out of tensor memory (32x32b.x32 loads) and subtracts it
+// from the front's lower triangle with coalesced accesses.
 //
 // Every wait on the completion barrier is bounded (2 s of %globaltimer): on
 // expiry the CTA records kTcErrWait, waits once more with the same bound, frees
