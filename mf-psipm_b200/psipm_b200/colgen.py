@@ -5,7 +5,7 @@ The reference's column-generation drivers (``retrospective_solve`` and
 restricted master LPs on a working set of columns with ``psipm_solve`` and
 price the remaining columns with the duals after each converged master.
 This module is the device counterpart of that loop in its basic form (no
-retrospective elimination, no warm start mapping between masters):
+retrospective elimination, no l1 budgets):
 
 * the first working set is the covering crash support when asked for and
   the LP is a covering LP (:func:`covering_crash`), else the free columns and
@@ -14,7 +14,8 @@ retrospective elimination, no warm start mapping between masters):
   artificial column ``+e_i`` and one ``-e_i`` per row at a large cost, so
   every master is feasible (the reference's ``cg_artificial_cost``);
 * each master is solved to ``tol`` by the device-resident PS-IPM
-  (``ipm_device.solve_standard``);
+  (``ipm_device.solve_standard``), from its own starting point or, when
+  asked for, from the previous master's solution mapped onto its columns;
 * pricing runs on the device over all columns (``pricing.DevicePricing``:
   ``A' y - c`` and the ``pricing_batch`` most violated columns not yet
   working), the same kernels as the HSD pricing round;
@@ -141,6 +142,49 @@ def covering_crash(lp) -> Optional[np.ndarray]:
     return working
 
 
+def mapped_master_start(lp, old_cols: np.ndarray, old_sol, new_cols: np.ndarray):
+    """A starting point for the next master from the last one's solution, as
+    the reference's ``_mapped_rmp_start`` (psipm_active_pool.py:3536-3599)
+    maps a restricted master across a change of support: columns kept from
+    the old master keep their x, z, w; the artificial columns (here 2m of
+    them, +e_i and -e_i, after the structural ones) keep theirs; y is kept; a
+    new column starts central at mu = max(old mu, 1e-10): x = max(sqrt(min(mu,
+    1)), 1e-8) (a boxed one inside [floor, u/2], floor = max(1e-12, 8 eps (1 +
+    |u|))), z = mu / x and, if boxed, w = mu / (u - x).  Returns (x, y, z, w)
+    for the new master, or None without an old solution."""
+    if old_sol is None or old_cols is None:
+        return None
+    m = lp.A.shape[0]
+    k_old, k_new = old_cols.size, new_cols.size
+    x = np.zeros(k_new + 2 * m)
+    z = np.zeros_like(x)
+    w = np.zeros_like(x)
+    loc = np.searchsorted(old_cols, new_cols)
+    common = (loc < k_old) & (old_cols[np.minimum(loc, max(0, k_old - 1))] == new_cols)
+    src = loc[common]
+    x[:k_new][common] = old_sol.x[src]
+    z[:k_new][common] = old_sol.z[src]
+    w[:k_new][common] = old_sol.w[src]
+    x[k_new:] = old_sol.x[k_old:]
+    z[k_new:] = old_sol.z[k_old:]
+    w[k_new:] = old_sol.w[k_old:]
+    fresh = np.flatnonzero(~common)
+    if fresh.size:
+        mu = max(float(old_sol.mu) if np.isfinite(old_sol.mu) else 0.0, 1e-10)
+        jj = new_cols[fresh]
+        xn = np.full(fresh.size, max(np.sqrt(min(mu, 1.0)), 1e-8))
+        boxed = np.asarray(lp.box, dtype=bool)[jj]
+        if boxed.any():
+            ub = lp.u[jj[boxed]]
+            floor = np.maximum(1e-12, _POS_FLOOR * (1.0 + np.abs(ub)))
+            xn[boxed] = np.minimum(np.maximum(xn[boxed], floor), 0.5 * ub)
+        x[fresh] = xn
+        z[fresh] = mu / np.maximum(xn, 1e-12)
+        if boxed.any():
+            w[fresh[boxed]] = mu / np.maximum(lp.u[jj[boxed]] - xn[boxed], 1e-12)
+    return x, np.array(old_sol.y, dtype=float), z, w
+
+
 def initial_working(lp, count: int) -> np.ndarray:
     """Free columns (never priced out) and the `count` cheapest others."""
     n = lp.A.shape[1]
@@ -168,10 +212,12 @@ def column_generation_solve(lp, tol: float = 1e-8, initial: Optional[int] = None
                             pricing_batch: Optional[int] = None, pricing_tol: Optional[float] = None,
                             max_rounds: int = 30, artificial_cost: Optional[float] = None,
                             device: int = 0, solver_options: Optional[dict] = None,
-                            crash: bool = False) -> ColumnGenerationResult:
+                            crash: bool = False, warm: bool = False) -> ColumnGenerationResult:
     """``crash=True`` starts a covering LP from :func:`covering_crash`'s
     feasible support (the reference's ``sparse_cover_crash``, on by default
-    there, psipm_active_pool.py:3746-3749), else from the cheapest columns."""
+    there, psipm_active_pool.py:3746-3749), else from the cheapest columns.
+    ``warm=True`` starts every master after the first from the previous
+    master's solution (:func:`mapped_master_start`)."""
     from .ipm_device import solve_standard
 
     started = time.perf_counter()
@@ -186,11 +232,15 @@ def column_generation_solve(lp, tol: float = 1e-8, initial: Optional[int] = None
     added = 0
     status, sol, cols = "round-limit", None, np.flatnonzero(working)
     try:
+        prev_cols, prev_sol = None, None
         for rnd in range(1, max_rounds + 1):
             cols = np.flatnonzero(working)
             master = _master(lp, cols, big)
-            sol, solver = solve_standard(master, tol=tol, device=device, solver_options=solver_options)
+            start = mapped_master_start(lp, prev_cols, prev_sol, cols) if warm else None
+            sol, solver = solve_standard(master, tol=tol, device=device, solver_options=solver_options,
+                                         initial=start)
             solver.close()
+            prev_cols, prev_sol = cols, sol
             if sol.status != "optimal":
                 status = f"master-{sol.status}"
                 break

@@ -62,6 +62,39 @@ class Solution:
     n_solve: int = 0
 
 
+def warm_start_point(lp, initial):
+    """The reference's safeguards on a caller's starting point
+    (psipm_active_pool.py:2527-2550): finite arrays of the LP's sizes; boxed x
+    kept at least the box floors inside [0, u] (floors min(8 eps, u/4) and
+    min(8 eps max(1, u), u/4)), nonnegative x at least 1e-12, z and w of
+    bounded entries at least 1e-12; free x as given, z zero off the
+    nonnegative entries and w zero off the boxed ones."""
+    if len(initial) != 4:
+        raise ValueError("initial must contain (x, y, z, w)")
+    x, y, z, w = (np.asarray(v, dtype=float).copy() for v in initial)
+    m, n = lp.A.shape
+    if x.size != n or y.size != m or z.size != n or w.size != n:
+        raise ValueError("warm-start dimensions do not match the LP")
+    if not all(np.isfinite(v).all() for v in (x, y, z, w)):
+        raise ValueError("warm start must be finite")
+    pos, box = np.asarray(lp.pos, dtype=bool), np.asarray(lp.box, dtype=bool)
+    lower = np.full(n, 1e-12)
+    if box.any():
+        ub = np.asarray(lp.u, dtype=float)[box]
+        quarter = 0.25 * ub
+        x_floor = np.minimum(8.0 * EPS, quarter)
+        s_floor = np.minimum(8.0 * EPS * np.maximum(1.0, ub), quarter)
+        lower[box] = x_floor
+        x[box] = np.minimum(np.maximum(x[box], x_floor), ub - s_floor)
+    x[pos] = np.maximum(x[pos], lower[pos])
+    z[pos] = np.maximum(z[pos], 1e-12)
+    w[box] = np.maximum(w[box], 1e-12)
+    x[~pos] = np.asarray(initial[0], dtype=float)[~pos]
+    z[~pos] = 0.0
+    w[~box] = 0.0
+    return x, y, z, w
+
+
 def starting_point_resident(dev, kkt, n: int) -> np.ndarray:
     """Device starting point: factor theta = 1, delta = 1 through the KKT
     policy (the reference's ``solver.factorize(ones, 1.0)``), the two
@@ -249,14 +282,16 @@ def prox_eval_resident(dev, kkt, npos_box, nbox, rho, delta, tol, maxit, pc, dea
 
 def psipm_solve_resident(lp, kkt_solver, tol=1e-6, maxit=200, inner_maxit=100, pc=3, rho=None, delta=None,
                          rf=1.0, ppm_red=0.5, compl="gap", tau=0.995, diverge_tol=1e4,
-                         time_limit=np.inf, max_outer: Optional[int] = None) -> Solution:
+                         time_limit=np.inf, max_outer: Optional[int] = None, initial=None) -> Solution:
     """Outer proximal loop (psipm_active_pool.py:2277-2788) on device-resident vectors.
 
     Arguments as the reference's ``psipm_solve`` with an external KKT solver
     (``max_outer``, not in the reference, stops after that many outer
-    iterations); ``kkt_solver`` must be a
-    :class:`GpuSpectralStableColumnPreconditioner`.
+    iterations; ``initial=(x, y, z, w)`` is the reference's warm start, taken
+    through :func:`warm_start_point` instead of the computed starting point);
+    ``kkt_solver`` must be a :class:`GpuSpectralStableColumnPreconditioner`.
     """
+    warm = None if initial is None else warm_start_point(lp, initial)
     if not isinstance(kkt_solver, GpuSpectralStableColumnPreconditioner):
         raise TypeError("the device-resident loop needs a GpuSpectralStableColumnPreconditioner")
     A = lp.A
@@ -279,9 +314,14 @@ def psipm_solve_resident(lp, kkt_solver, tol=1e-6, maxit=200, inner_maxit=100, p
     deadline = tic + time_limit
     dev.ipm_load(c, b, u, lp.pos, lp.box)
     solver.resident = True
-    starting_point_resident(dev, solver, n)
+    if warm is None:
+        starting_point_resident(dev, solver, n)
+        solver.h2d_bytes += 8 * n  # theta = 1
+    else:
+        dev.ipm_put(0, *warm)
+        solver.h2d_bytes += 8 * (3 * n + m)
     dev.ipm_copy(True)  # centre = iterate
-    solver.h2d_bytes += 8 * (2 * n + m) + 2 * n + 8 * n  # c, u, b, masks, theta = 1
+    solver.h2d_bytes += 8 * (2 * n + m) + 2 * n  # c, u, b, masks
     best_mu = np.inf
     sol = Solution(x=None, y=None, z=None, w=None)
     inner_tot = 0

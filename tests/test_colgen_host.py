@@ -58,3 +58,31 @@ def test_crash_support_is_feasible(name):
     assert np.all(r <= 1e-12 * (1 + np.abs(lp.b)))
     rows = A.indices[A.indptr[surplus]]
     assert np.unique(rows).size == lp.A.shape[0]
+
+
+def test_mapped_master_start():
+    """Kept columns and the artificials keep their values, new columns start
+    central (boxed ones inside their box), y is kept."""
+    from types import SimpleNamespace
+
+    from psipm_b200.colgen import mapped_master_start
+
+    lp = synthetic.set_cover(30, 400, seed=7)
+    m = lp.A.shape[0]
+    rng = np.random.default_rng(1)
+    old_cols = np.array([2, 5, 9, 40, 41, 77], dtype=np.int64)
+    new_cols = np.array([2, 3, 9, 41, 77, 100, 350], dtype=np.int64)
+    k = old_cols.size + 2 * m
+    old = SimpleNamespace(x=rng.uniform(0.1, 0.9, k), z=rng.uniform(0.1, 2, k), w=rng.uniform(0.1, 2, k),
+                          y=rng.standard_normal(m), mu=0.04)
+    x, y, z, w = mapped_master_start(lp, old_cols, old, new_cols)
+    assert x.size == new_cols.size + 2 * m and np.array_equal(y, old.y)
+    for a, j in enumerate(new_cols):
+        hit = np.flatnonzero(old_cols == j)
+        if hit.size:
+            assert (x[a], z[a], w[a]) == (old.x[hit[0]], old.z[hit[0]], old.w[hit[0]])
+        else:
+            assert x[a] == pytest.approx(0.2) and z[a] == pytest.approx(0.04 / 0.2)
+            assert (w[a] > 0) == bool(lp.box[j])
+    assert np.array_equal(x[new_cols.size:], old.x[old_cols.size:])
+    assert mapped_master_start(lp, None, None, new_cols) is None

@@ -74,3 +74,48 @@ def test_resident_loop_needs_the_spectral_solver():
     plain = GpuStableActiveColumnPreconditioner(lp.A, protected=~lp.pos, dev=FakeDevice(lp.A), **OPTS)
     with pytest.raises(TypeError):
         psipm_solve_resident(lp, plain, tol=1e-8)
+
+
+def test_warm_start_from_a_solution_converges_at_once():
+    """initial=(x, y, z, w) (the reference's warm start, psipm_active_pool.py:
+    2527-2550) from a converged solution: the same objective in a few outer
+    iterations instead of the cold start's."""
+    lp = LPS["random"]()
+    cold = psipm_solve_resident(lp, make(lp, FakeDevice(lp.A)), tol=1e-8)
+    assert cold.status == "optimal"
+    warm = psipm_solve_resident(lp, make(lp, FakeDevice(lp.A)), tol=1e-8,
+                                initial=(cold.x, cold.y, cold.z, cold.w))
+    assert warm.status == "optimal"
+    assert warm.outer_iter < cold.outer_iter
+    assert abs(warm.obj - cold.obj) <= 1e-8 * max(1.0, abs(cold.obj))
+
+
+def test_warm_start_safeguards():
+    from psipm_b200.ipm_device import warm_start_point
+
+    lp = synthetic.random_lp(20, 60, seed=4)
+    rng = np.random.default_rng(0)
+    n, m = lp.A.shape[1], lp.A.shape[0]
+    lp.pos[:5] = False  # free columns
+    lp.box[5:15] = True
+    lp.u[5:15] = np.linspace(1e-17, 2.0, 10)
+    lp.box[:5] = False
+    x, y, z, w = rng.standard_normal(n), rng.standard_normal(m), rng.standard_normal(n), rng.standard_normal(n)
+    x[5:15] = np.linspace(-1.0, 3.0, 10)
+    xs, ys, zs, ws = warm_start_point(lp, (x, y, z, w))
+    eps = np.finfo(float).eps
+    ub = lp.u[5:15]
+    x_floor = np.minimum(8 * eps, 0.25 * ub)
+    s_floor = np.minimum(8 * eps * np.maximum(1.0, ub), 0.25 * ub)
+    assert np.array_equal(xs[5:15], np.maximum(np.minimum(np.maximum(x[5:15], x_floor), ub - s_floor), x_floor))
+    assert np.array_equal(xs[:5], x[:5]) and np.all(zs[:5] == 0.0) and np.all(ws[~lp.box] == 0.0)
+    assert np.all(xs[lp.pos & ~lp.box] >= 1e-12) and np.all(zs[lp.pos] >= 1e-12) and np.all(ws[lp.box] >= 1e-12)
+    assert np.array_equal(ys, y)
+    with pytest.raises(ValueError):
+        warm_start_point(lp, (x, y, z))
+    with pytest.raises(ValueError):
+        warm_start_point(lp, (x[:-1], y, z, w))
+    bad = x.copy()
+    bad[7] = np.nan
+    with pytest.raises(ValueError):
+        warm_start_point(lp, (bad, y, z, w))
