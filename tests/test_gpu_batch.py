@@ -5,7 +5,6 @@ against the same LPs solved one after another: every LP optimal in both, the
 same objective to 1e-8 relative, and the batch's throughput reported next to
 the sequential one."""
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
