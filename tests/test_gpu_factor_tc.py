@@ -12,7 +12,6 @@ amplified by the conditioning) and as the FP64 factor, and a full FP32 solve
 reaches the FP64 solve's objective.
 """
 
-
 import numpy as np
 import pytest
 
